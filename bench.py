@@ -1,0 +1,421 @@
+"""GRG up+down throughput benchmark of the B200 backend (one JSON line on rank 0).
+
+Workload: the synthetic GRG with the shape of the "plain FP64 drop-in on B200" configuration
+(100k haploid samples, 40 internal levels, ~5M nodes, ~60M edges, 1M mutations, 1% missing
+entries via per-mutation missingness nodes), fully resident, FP64, k right-hand sides.  One
+step = one ``up`` traversal (X·G) of a resident sample-major input followed by one ``down``
+traversal (X·Gᵀ, with the miss input) that consumes the up output in place (the prepared
+ops' shared ``io0`` buffer).  Metric: edge·RHS/s = steps · 2·E·k / device time.
+
+* ``value``: device time of K steps (CUDA events on the caller stream, inputs resident);
+  the working set (~0.8 GB of gather lists and node rows) exceeds the 126 MB L2, so no L2
+  flush is needed between steps.
+* ``e2e``: the same steps through the public prepared-op API with the inputs copied from
+  pinned host memory and both outputs copied back every step.
+* ``roofline``: the level gather kernels timed live (events around every level launch of one
+  instrumented up+down pass); algorithmic bytes per traversal as in DESIGN.md.
+* ``cpu_baseline``: the oracle (SciPy restatement of the reference's ReferenceRuntime) on one
+  step of the same graph, rank 0, N=1 only.
+* ``--impl reference``: the reference's CPU path (the oracle port; the pure-Python reference
+  cannot be installed offline) timed on the same workload.
+
+Multi-GPU (``torchrun``): every rank runs its own graph (a different seed, as a genomic region
+would be), no data-path collective; ``value`` sums the ranks' work over the max of their times.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import dataclasses
+import json
+import os
+from pathlib import Path
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "GRG up+down edge·RHS/s (k RHS, FP64)"
+UNIT = "edge·RHS/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--k", type=int, default=8)
+    p.add_argument("--workload", choices=["config2", "small"], default="config2")
+    p.add_argument("--exact-order", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--artifact", default=None, help="reuse an existing .grg_spmv instead of generating one")
+    return p.parse_args()
+
+
+def workload_spec(name: str, seed: int):
+    from grg_spmv_b200.synth import CONFIG2, SynthSpec
+
+    if name == "config2":
+        return dataclasses.replace(CONFIG2, seed=seed)
+    return SynthSpec(num_samples=20_000, num_levels=20, num_nodes=600_000, num_mutations=100_000, children=(2, 28),
+                     miss_fraction=0.01, seed=seed)
+
+
+def make_artifact(args, rank: int) -> tuple[Path, float]:
+    from grg_spmv_b200.synth import write_synthetic_artifact
+
+    if args.artifact:
+        return Path(args.artifact), 0.0
+    out = Path(tempfile.mkdtemp(prefix="grg_bench_")) / f"{args.workload}_r{rank}.grg_spmv"
+    t0 = time.perf_counter()
+    write_synthetic_artifact(workload_spec(args.workload, seed=rank), out)
+    return out, time.perf_counter() - t0
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def wait_for_samples(self, count: int = 2, timeout_s: float = 3.0) -> None:
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < timeout_s:
+            if self.path.exists() and len(self.path.read_text().splitlines()) >= count:
+                return
+            time.sleep(0.05)
+
+    def summary(self) -> dict:
+        rows = []
+        for line in self.path.read_text().splitlines() if self.path.exists() else []:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][2]) if rows else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak_hbm() -> tuple[float, str]:
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        try:
+            return float(json.loads(path.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def level_bytes(levels, k: int, itemsize: int, direction: str, num_mutations: int, use_miss: bool) -> int:
+    """Algorithmic bytes of one traversal's level kernels: each gather entry (4 B) and row
+    pointer (4 B) read once, each destination row written once and read once by later levels
+    or the output stage (2·k·b), plus (down) the mutation inputs read once."""
+    total = 0
+    for lv in levels:
+        total += 4 * int(lv.num_entries) + 4 * (int(lv.num_rows) + 1) + 2 * int(lv.num_rows) * k * itemsize
+    if direction == "down":
+        total += num_mutations * k * itemsize * (2 if use_miss else 1)
+    return total
+
+
+def run_b200(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local_rank))
+    device = torch.device("cuda", local_rank)
+    torch.cuda.set_device(device)
+
+    from grg_spmv_b200 import RuntimeRequirements, scan_grg_spmv
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime, plan_b200_layout
+    from grg_spmv_b200.backends.b200 import _native as nat
+
+    path, gen_s = make_artifact(args, rank)
+    scan = scan_grg_spmv(path)
+    k = int(args.k)
+    req = RuntimeRequirements(max_k_up=k, max_k_down=k, need_down_miss_input=True, need_up_miss_output=False,
+                              need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
+    pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order), plan_down=B200Plan(exact_order=args.exact_order))
+    stream = torch.cuda.Stream(device=device)
+    layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
+                              device=local_rank, stream=stream, pair=pair)
+    t0 = time.perf_counter()
+    runtime = B200Runtime(layout).__enter__()
+    enter_s = time.perf_counter() - t0
+    (grg,) = runtime.grgs
+    S, M, E = grg.num_samples, grg.num_mutations, grg.num_edges
+    rng = np.random.default_rng(100 + rank)
+    x_up_np = rng.standard_normal((k, S))
+    miss_np = rng.choice(np.asarray([0.0, 1.0]), size=(k, M), p=[0.99, 0.01])
+    with torch.cuda.device(device), torch.cuda.stream(stream):
+        up = grg.prepare_matmul_cuda(direction="up", k=k)
+        down = grg.prepare_matmul_cuda(direction="down", k=k, use_miss=True)
+        x_up = torch.from_numpy(x_up_np).to(device)
+        down.miss_input.copy_(torch.from_numpy(miss_np).to(device))
+    assert up.output.data_ptr() == down.input.data_ptr()
+
+    def step():
+        up.input.copy_(x_up)
+        up()
+        down()
+
+    def synced_barrier():
+        torch.cuda.synchronize(device)
+        if world > 1:
+            dist.barrier()
+
+    with torch.cuda.device(device), torch.cuda.stream(stream):
+        for _ in range(max(args.warmup, 0)):
+            step()
+        synced_barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+        def busy(seconds: float) -> None:  # untimed load so the clock samples see the GPU busy
+            t0 = time.perf_counter()
+            while time.perf_counter() - t0 < seconds:
+                for _ in range(4):
+                    step()
+                torch.cuda.synchronize(device)
+
+        with ClockSampler(local_rank) as clocks:
+            clocks.wait_for_samples(1)
+            busy(0.6)
+            synced_barrier()
+            start.record(stream)
+            for _ in range(args.steps):
+                step()
+            end.record(stream)
+            synced_barrier()
+            busy(0.6)
+        elapsed_ms = start.elapsed_time(end)
+    max_ms = elapsed_ms
+    total_work = args.steps * 2.0 * E * k
+    if world > 1:
+        t = torch.tensor([elapsed_ms, total_work], device=device, dtype=torch.float64)
+        mx = t.clone()
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        max_ms, total_work = float(mx[0]), float(t[1])
+    value = total_work / (max_ms / 1e3)
+
+    # Live per-kernel timing of the level gathers (one instrumented up+down pass).
+    lib = runtime._lib
+    level_ms = {"up": 0.0, "down": 0.0}
+    level_launches = 0
+    lv_bytes = 0
+    with torch.cuda.device(device), torch.cuda.stream(stream):
+        up.input.copy_(x_up)
+        for name, op in (("up", up), ("down", down)):
+            args_c = op._args
+            if name == "up":
+                nat.check(lib, lib.grg_b200_seed_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "seed_up")
+            levels = runtime._artifacts[0].levels[op._spec.direction]
+            evs = []
+            for i in range(levels.count):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                nat.check(lib, lib.grg_b200_run_level(ctypes.byref(args_c), ctypes.byref(levels.array[i]),
+                                                      ctypes.c_void_p(stream.cuda_stream)), "run_level")
+                b.record(stream)
+                evs.append((a, b))
+                level_launches += 1 + (1 if levels.array[i].num_heavy > 0 else 0)
+            if name == "up":
+                nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
+            else:
+                nat.check(lib, lib.grg_b200_output_down(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_down")
+            torch.cuda.synchronize(device)
+            level_ms[name] = sum(a.elapsed_time(b) for a, b in evs)
+            for (a, b), lv in zip(evs, list(levels.array)):
+                ms = a.elapsed_time(b)
+                nbytes = level_bytes([lv], k, 8, "up", M, False)
+                print(f"[level] {name} rows={lv.num_rows} entries={lv.num_entries} heavy={lv.num_heavy} "
+                      f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
+            lv_bytes += level_bytes(list(levels.array), k, 8, name, M, use_miss=True)
+    launches_per_step = level_launches + 1 + 1 + 1  # + seed_up + output_up + output_down
+    level_total_ms = level_ms["up"] + level_ms["down"]
+    peak, peak_kind = measured_peak_hbm()
+    achieved = lv_bytes / (level_total_ms / 1e3) / 1e9
+
+    # End-to-end through the public API with pinned host buffers.
+    e2e = None
+    if not args.no_e2e:
+        x_host = torch.from_numpy(x_up_np).pin_memory()
+        miss_host = torch.from_numpy(miss_np).pin_memory()
+        out_up_host = torch.empty((k, M), dtype=torch.float64).pin_memory()
+        out_down_host = torch.empty((k, S), dtype=torch.float64).pin_memory()
+        with torch.cuda.device(device), torch.cuda.stream(stream):
+            def e2e_step():
+                up.input.copy_(x_host, non_blocking=True)
+                up()
+                out_up_host.copy_(up.output, non_blocking=True)
+                down.miss_input.copy_(miss_host, non_blocking=True)
+                down()
+                out_down_host.copy_(down.output, non_blocking=True)
+
+            for _ in range(max(args.warmup, 1)):
+                e2e_step()
+            synced_barrier()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.steps):
+                e2e_step()
+            b.record(stream)
+            synced_barrier()
+            e2e_ms = a.elapsed_time(b)
+        if world > 1:
+            t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t[0])
+        e2e = {"value": total_work / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms / args.steps,
+               "h2d_bytes_per_step": int((S + M) * k * 8), "d2h_bytes_per_step": int((M + S) * k * 8)}
+
+    # CPU baseline (oracle) and a parity spot check of the same step, rank 0 at N=1.
+    cpu = None
+    max_rel = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(REPO / "oracle"))
+        from grg_oracle import OracleGRG
+
+        oracle = OracleGRG(path)
+        t0 = time.perf_counter()
+        ref_up = oracle.matmul(x_up_np, "up")
+        ref_down = oracle.matmul(ref_up, "down", miss=miss_np.copy())
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": 2.0 * E * k / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"1 up+down step (k={k}) of the same graph; SciPy ReferenceRuntime restatement, 1 thread",
+               "seconds": cpu_s}
+        with torch.cuda.device(device), torch.cuda.stream(stream):
+            up.input.copy_(x_up)
+            up()
+            got_up = up.output.cpu().numpy()
+            down()
+            got_down = down.output.cpu().numpy()
+        rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-300))
+        max_rel = max(rel(got_up, ref_up), rel(got_down, ref_down))
+
+    runtime.__exit__(None, None, None)
+    if rank == 0:
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded generator with the configuration's shapes; no public GRG dataset offline)",
+            "config": {"workload": f"{args.workload}: S={S}, levels={scan.num_levels}, N={grg.num_nodes}, E={E}, M={M}, "
+                                   f"1% missing, fully resident, up+down per step",
+                       "k": k, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
+                       "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
+                       "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "level gather (level_narrow_kernel + level_wide_kernel)",
+                         "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
+                         "level_ms_per_step": level_total_ms, "level_bytes_per_step": lv_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches_per_step * args.steps),
+            "clocks": clocks.summary(),
+            "max_rel_err_vs_oracle": max_rel,
+            "setup_s": {"generate": gen_s, "runtime_enter": enter_s},
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def run_reference(args) -> None:
+    """The reference's CPU path (oracle port of ReferenceRuntime) on the same workload."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, str(REPO / "oracle"))
+    from grg_oracle import OracleGRG
+
+    path, _ = make_artifact(args, 0)
+    oracle = OracleGRG(path)
+    k = int(args.k)
+    rng = np.random.default_rng(100)
+    x = rng.standard_normal((k, oracle.num_samples))
+    miss = rng.choice(np.asarray([0.0, 1.0]), size=(k, oracle.num_mutations), p=[0.99, 0.01])
+
+    def step():
+        mid = oracle.matmul(x, "up")
+        oracle.matmul(mid, "down", miss=miss.copy())
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    secs = time.perf_counter() - t0
+    value = args.steps * 2.0 * oracle.num_edges * k / secs
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}", "k": k, "num_edges": oracle.num_edges},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
+                         "sample": "full up+down steps; SciPy restatement of ReferenceRuntime (single-threaded)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def main() -> None:
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,204 @@
+"""Host-side construction of the per-level gather lists that the B200 kernels walk.
+
+For every destination level the traversal needs, for each row, the list of rows it adds up.
+The lists are built from the artifact's ``A_blocks`` and selectors and ordered so that a
+left-to-right sum with a fresh partial sum per segment reproduces ``ReferenceRuntime``:
+
+* up, level ``L >= 1``: the row's children, one segment per child level in ascending level
+  order, ascending node id inside a segment (``dst += A[L][src] @ v[src]`` for ``src``
+  ascending, ``pygrgl_spmv/backends/reference.py:399-407``; CSR rows summed left to right).
+* down, every level from the top down: first the row's mutations (``sel_mut^T x``, ascending
+  mutation id, duplicates kept, ``reference.py:416-417``), then its missingness mutations
+  (``sel_miss^T miss``, ``:418-419``), then its parents, one segment per parent level in
+  descending level order, ascending id inside a segment (``A[src][D].T @ v[src]`` for ``src``
+  descending, ``:420-429`` with ``pygrgl_spmv/backends/base.py:115-117``; a CSC product adds
+  columns in ascending order).
+
+Blocks are canonicalised first (duplicates merged, columns sorted), as the reference does in
+``materialize_sparse_block`` (``pygrgl_spmv/backends/base.py:128-139``).  Each level is packed
+into one byte blob ``[int32 row_ptr | int32 heavy_rows | uint32 entries]`` with 16-byte
+aligned sections, the unit of residency and of streaming through the ring.
+"""
+
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from grg_spmv_b200.backends.b200 import _native as nat
+
+ALIGN = 16
+
+
+def _align(n: int) -> int:
+    return (int(n) + ALIGN - 1) // ALIGN * ALIGN
+
+
+def blob_layout(num_rows: int, num_heavy: int, num_entries: int) -> tuple[int, int, int, int]:
+    """(off_row_ptr, off_heavy, off_entries, blob_bytes) of a level blob."""
+    off_heavy = _align(4 * (int(num_rows) + 1))
+    off_entries = off_heavy + _align(4 * int(num_heavy))
+    return 0, off_heavy, off_entries, off_entries + _align(4 * max(int(num_entries), 1))
+
+
+@dataclass
+class LevelGather:
+    level: int
+    row_begin: int
+    num_rows: int
+    row_ptr: np.ndarray  # int32 [num_rows + 1]
+    entries: np.ndarray  # uint32
+    heavy_rows: np.ndarray  # int32
+    heavy_threshold: int
+
+    @property
+    def num_entries(self) -> int:
+        return int(self.entries.size)
+
+    def layout(self) -> tuple[int, int, int, int]:
+        return blob_layout(self.num_rows, self.heavy_rows.size, self.entries.size)
+
+    def pack(self) -> np.ndarray:
+        off_ptr, off_heavy, off_entries, nbytes = self.layout()
+        blob = np.zeros(nbytes, dtype=np.uint8)
+        blob[off_ptr:off_ptr + 4 * self.row_ptr.size] = self.row_ptr.view(np.uint8)
+        blob[off_heavy:off_heavy + 4 * self.heavy_rows.size] = self.heavy_rows.view(np.uint8)
+        blob[off_entries:off_entries + 4 * self.entries.size] = self.entries.view(np.uint8)
+        return blob
+
+
+def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.ndarray, np.ndarray]:
+    """(rows, cols) of a 0/1 CSR block, sorted by (row, col) with duplicates merged."""
+    nrows, ncols = int(shape[0]), int(shape[1])
+    ptr = np.asarray(indptr, dtype=np.int64)
+    cols = np.asarray(indices, dtype=np.int64)
+    rows = np.repeat(np.arange(nrows, dtype=np.int64), np.diff(ptr))
+    key = rows * max(ncols, 1) + cols
+    if key.size > 1 and not np.all(key[1:] > key[:-1]):
+        key = np.unique(key)
+        rows, cols = key // max(ncols, 1), key % max(ncols, 1)
+    return rows, cols
+
+
+def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
+            group: np.ndarray, heavy_threshold: int) -> LevelGather:
+    """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr."""
+    order = np.argsort(rows, kind="stable")
+    rows, ids, src, group = rows[order], ids[order], src[order], group[order]
+    if ids.size and int(ids.max()) > nat.MAX_ID:
+        raise ValueError(f"level {level} names ids above {nat.MAX_ID}, beyond the B200 backend's limit")
+    counts = np.bincount(rows, minlength=num_rows) if rows.size else np.zeros(num_rows, dtype=np.int64)
+    row_ptr = np.zeros(num_rows + 1, dtype=np.int64)
+    np.cumsum(counts, out=row_ptr[1:])
+    if row_ptr[-1] > np.iinfo(np.int32).max:
+        raise ValueError(f"level {level} has {int(row_ptr[-1])} entries, above the 2^31-1 per-level limit")
+    start = np.ones(ids.size, dtype=bool)
+    if ids.size > 1:
+        start[1:] = (rows[1:] != rows[:-1]) | (group[1:] != group[:-1])
+    entries = (ids.astype(np.uint32) | (src.astype(np.uint32) << np.uint32(nat.SRC_SHIFT))
+               | np.where(start, np.uint32(nat.SEG_START), np.uint32(0)))
+    heavy = np.flatnonzero(counts > heavy_threshold).astype(np.int32)
+    return LevelGather(level, int(row_begin), int(num_rows), row_ptr.astype(np.int32), entries.astype(np.uint32),
+                       heavy, int(heavy_threshold))
+
+
+def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
+    """Canonical COO of every non-empty block, keyed by (dst level, src level)."""
+    out = {}
+    for block in blocks:
+        if block.nnz == 0:
+            continue
+        out[(block.dst_level, block.src_level)] = canonical_coo(block.indices, block.indptr, block.shape)
+    return out
+
+
+def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int) -> list[LevelGather]:
+    """Gather lists for up levels 1..h-1 (level 0 is seeded from the input)."""
+    off = np.asarray(level_offsets, dtype=np.int64)
+    h = off.size - 1
+    levels = []
+    for dst in range(1, h):
+        n = int(off[dst + 1] - off[dst])
+        rows, ids, src = [], [], []
+        for s in range(dst):
+            if (dst, s) not in coo:
+                continue
+            r, c = coo[(dst, s)]
+            rows.append(r)
+            ids.append(c + off[s])
+            src.append(np.full(r.size, s, dtype=np.int16))
+        cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
+        r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
+        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold))
+    return levels
+
+
+def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[np.ndarray, np.ndarray]:
+    """(node, mutation) pairs of a selector sorted by node, ascending mutation inside a node."""
+    ptr = np.asarray(ptr, dtype=np.int64)
+    muts = np.repeat(np.arange(num_rows, dtype=np.int64), np.diff(ptr))
+    nodes = np.asarray(idx, dtype=np.int64)
+    order = np.argsort(nodes, kind="stable")
+    return nodes[order], muts[order]
+
+
+def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int) -> list[LevelGather]:
+    """Gather lists for down levels h-1..0 in execution order.
+
+    ``sel_mut``/``sel_miss`` are (indptr, indices, num_mutations) triples; ``sel_miss`` may be
+    None when no miss input is needed.
+    """
+    off = np.asarray(level_offsets, dtype=np.int64)
+    h = off.size - 1
+    mut_nodes, mut_ids = _selector_by_node(sel_mut[0], sel_mut[1], sel_mut[2])
+    miss_nodes, miss_ids = (None, None) if sel_miss is None else _selector_by_node(sel_miss[0], sel_miss[1], sel_miss[2])
+    levels = []
+    for dst in range(h - 1, -1, -1):
+        lo, hi = int(off[dst]), int(off[dst + 1])
+        rows, ids, src, grp = [], [], [], []
+        for nodes, mids, code, g in ((mut_nodes, mut_ids, nat.SRC_INPUT, 0), (miss_nodes, miss_ids, nat.SRC_MISS, 1)):
+            if nodes is None:
+                continue
+            a, b = np.searchsorted(nodes, [lo, hi])
+            rows.append(nodes[a:b] - lo)
+            ids.append(mids[a:b])
+            src.append(np.full(b - a, code, dtype=np.uint8))
+            grp.append(np.full(b - a, g, dtype=np.int16))
+        for s in range(h - 1, dst, -1):
+            if (s, dst) not in coo:
+                continue
+            p, c = coo[(s, dst)]  # rows: parents (level s), cols: children (level dst)
+            order = np.argsort(c, kind="stable")
+            rows.append(c[order])
+            ids.append(p[order] + off[s])
+            src.append(np.zeros(p.size, dtype=np.uint8))
+            grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
+        cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
+        levels.append(_finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
+                              cat(grp, np.int16), heavy_threshold))
+    return levels
+
+
+def up_entry_bound(scan, level: int) -> int:
+    return int(sum(b.nnz for b in scan.blocks if b.dst_level == level))
+
+
+def down_entry_bound(scan, level: int, with_miss: bool) -> int:
+    total = sum(b.nnz for b in scan.blocks if b.src_level == level)
+    total += int(scan.selector_nnz_by_level[level, 0])
+    if with_miss:
+        total += int(scan.selector_nnz_by_level[level, 1])
+    return int(total)
+
+
+__all__ = [
+    "LevelGather",
+    "blob_layout",
+    "build_down_levels",
+    "build_up_levels",
+    "canonical_coo",
+    "down_entry_bound",
+    "load_blocks",
+    "up_entry_bound",
+]

@@ -1,0 +1,873 @@
+// libgrg_b200: GRG up/down traversal kernels for NVIDIA B200 (sm_100a) behind a C ABI.
+//
+// The operand of a GRG traversal is a 0/1 DAG, so each level is a gather-sum: every
+// destination row adds up the rows it points at.  There is no dense contraction, so the
+// tensor cores have nothing to do; the kernels are bound by HBM/L2 traffic (the gather list
+// is streamed once, node rows are read once per edge and written once).  Design:
+//
+//  * One pass per destination level, atomic-free: up gathers each node's children, down
+//    gathers each node's parents (the reference's Triton CSC kernel scatters with atomics
+//    instead, pygrgl_spmv/backends/triton/kernel.py:101-138).  Results are deterministic.
+//  * Narrow rows: a group of G lanes owns one row; each lane holds V consecutive columns
+//    (double2 / float4 vector loads), so a warp covers 32/G rows and the k columns of a row
+//    are read as one contiguous segment.  The lane sums the row's list left to right, one
+//    segment at a time, exactly like ReferenceRuntime (one sparse product per source level
+//    added to the destination, pygrgl_spmv/backends/reference.py:396-429).
+//  * Heavy rows (more than heavy_threshold entries; down-direction samples can have
+//    thousands of parents) get one 128-thread CTA each.  Default: entries are split over
+//    the CTA and tree-reduced in a fixed order (deterministic, exact for integer-valued
+//    inputs).  exact_order=1: the CTA loads chunks in parallel and one thread group adds them
+//    in list order, which is bit-identical to the reference for any input.
+//  * Down seeding (sel_mut^T x and sel_miss^T miss, the reference's atomic index_add_ at
+//    triton/backend.py:1143-1150) is folded into the level lists as leading INPUT/MISS
+//    segments, so it costs no extra pass; up seeding touches level 0 only.
+//  * Streamed levels are copied from pinned host memory into device ring slots on a copy
+//    stream, ordered with per-slot events, so copies overlap the previous levels' compute.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <type_traits>
+
+#include "grg_b200.h"
+
+namespace {
+
+thread_local char g_last_error[1024] = "";
+
+int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define GRG_CUDA_TRY(expr)                                                                  \
+    do {                                                                                    \
+        cudaError_t err__ = (expr);                                                         \
+        if (err__ != cudaSuccess)                                                           \
+            return fail(GRG_B200_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(err__)); \
+    } while (0)
+
+#define GRG_LAUNCH_CHECK(name)                                                              \
+    do {                                                                                    \
+        cudaError_t err__ = cudaGetLastError();                                             \
+        if (err__ != cudaSuccess)                                                           \
+            return fail(GRG_B200_ERR_CUDA, "launch of %s failed: %s", name, cudaGetErrorString(err__)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------------------
+// Vector packs
+// ---------------------------------------------------------------------------------------
+template <typename T, int V>
+struct alignas(sizeof(T) * V) Pack {
+    T v[V];
+};
+
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> zero_pack() {
+    Pack<T, V> r;
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = T(0);
+    return r;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> splat(T x) {
+    Pack<T, V> r;
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = x;
+    return r;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void add_into(Pack<T, V>& a, const Pack<T, V>& b) {
+#pragma unroll
+    for (int i = 0; i < V; ++i) a.v[i] = a.v[i] + b.v[i];
+}
+
+// Read-only (non-coherent) load: every row read by a kernel was written by an earlier launch.
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> ld_ro(const T* p) {
+    Pack<T, V> r;
+    if constexpr (V == 1) {
+        r.v[0] = __ldg(p);
+    } else if constexpr (std::is_same<T, double>::value && V == 2) {
+        const double2 d = __ldg(reinterpret_cast<const double2*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else if constexpr (std::is_same<T, float>::value && V == 2) {
+        const float2 d = __ldg(reinterpret_cast<const float2*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else {
+        static_assert(std::is_same<T, float>::value && V == 4, "unsupported pack");
+        const float4 d = __ldg(reinterpret_cast<const float4*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+        r.v[2] = d.z;
+        r.v[3] = d.w;
+    }
+    return r;
+}
+
+template <typename T, int V>
+__device__ __forceinline__ void st_pack(T* p, const Pack<T, V>& x) {
+    *reinterpret_cast<Pack<T, V>*>(p) = x;
+}
+
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// ---------------------------------------------------------------------------------------
+// Kernel parameters
+// ---------------------------------------------------------------------------------------
+struct LevelArgs {
+    int64_t row_begin;
+    int64_t num_rows;
+    const int32_t* row_ptr;
+    const uint32_t* entries;
+    const int32_t* heavy_rows;
+    int64_t num_heavy;
+    int32_t heavy_threshold;
+    int32_t use_miss;
+    void* state;
+    int64_t ld_state;
+    const void* x;
+    int64_t ld_x;
+    const void* miss;
+    int64_t ld_miss;
+    const void* init_vector;
+    const void* init_matrix;
+    int64_t ld_init;
+    const int32_t* node_perm;
+    const void* xtx_node;
+    int64_t k;
+    int32_t log2g;
+    int32_t* err;
+    int64_t lim_state;
+    int64_t lim_x;
+    int64_t lim_miss;
+};
+
+enum DeviceError : int32_t {
+    kErrStateId = 1,
+    kErrInputId = 2,
+    kErrMissId = 3,
+    kErrPerm = 4,
+    kErrSelector = 5,
+};
+
+__device__ __forceinline__ void report(int32_t* err, int32_t code) {
+    if (err) atomicCAS(err, 0, code);
+}
+
+template <typename T, int V, int INIT>
+__device__ __forceinline__ Pack<T, V> init_value(const LevelArgs& a, int64_t row, int64_t c) {
+    if constexpr (INIT == GRG_B200_INIT_VECTOR) {
+        return ld_ro<T, V>(static_cast<const T*>(a.init_vector) + c);
+    } else if constexpr (INIT == GRG_B200_INIT_XTX) {
+        return splat<T, V>(__ldg(static_cast<const T*>(a.xtx_node) + row));
+    } else if constexpr (INIT == GRG_B200_INIT_MATRIX) {
+        const int64_t orig = __ldg(a.node_perm + row);
+        if (a.err && (orig < 0 || orig >= a.lim_state)) {
+            report(a.err, kErrPerm);
+            return zero_pack<T, V>();
+        }
+        return ld_ro<T, V>(static_cast<const T*>(a.init_matrix) + orig * a.ld_init + c);
+    } else {
+        return zero_pack<T, V>();
+    }
+}
+
+// Address of the row named by a coded entry; nullptr when the entry is skipped.
+template <typename T>
+__device__ __forceinline__ const T* entry_row(const LevelArgs& a, uint32_t code) {
+    const uint32_t src = (code >> GRG_B200_SRC_SHIFT) & GRG_B200_SRC_MASK;
+    const int64_t id = code & GRG_B200_ID_MASK;
+    if (src == GRG_B200_SRC_STATE) {
+        if (a.err && id >= a.lim_state) {
+            report(a.err, kErrStateId);
+            return nullptr;
+        }
+        return static_cast<const T*>(a.state) + id * a.ld_state;
+    }
+    if (src == GRG_B200_SRC_INPUT) {
+        if (a.err && id >= a.lim_x) {
+            report(a.err, kErrInputId);
+            return nullptr;
+        }
+        return static_cast<const T*>(a.x) + id * a.ld_x;
+    }
+    if (!a.use_miss) return nullptr;
+    if (a.err && id >= a.lim_miss) {
+        report(a.err, kErrMissId);
+        return nullptr;
+    }
+    return static_cast<const T*>(a.miss) + id * a.ld_miss;
+}
+
+// ---------------------------------------------------------------------------------------
+// Level kernels
+// ---------------------------------------------------------------------------------------
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(256) level_narrow_kernel(LevelArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t local = t >> a.log2g;
+    if (local >= a.num_rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    const int32_t e0 = __ldg(a.row_ptr + local);
+    const int32_t e1 = __ldg(a.row_ptr + local + 1);
+    if (e1 - e0 > a.heavy_threshold) return;  // handled by level_wide_kernel
+    const int64_t row = a.row_begin + local;
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    // Entries are consumed U at a time: all U codes are loaded, then all U rows, then the U
+    // values are added in list order.  The adds keep the reference's order; the loads of a
+    // chunk are independent, so U row fetches are in flight per lane instead of one.
+    constexpr int U = (V == 1) ? 8 : 4;
+    for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step) {
+        Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+        Pack<T, V> seg = zero_pack<T, V>();
+        for (int32_t e = e0; e < e1; e += U) {
+            uint32_t code[U];
+            Pack<T, V> val[U];
+            bool valid[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) code[u] = (e + u < e1) ? __ldg(a.entries + e + u) : 0u;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const T* src = (e + u < e1) ? entry_row<T>(a, code[u]) : nullptr;
+                valid[u] = src != nullptr;
+                val[u] = valid[u] ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (code[u] & GRG_B200_SEG_START) {
+                    add_into(acc, seg);
+                    seg = zero_pack<T, V>();
+                }
+                if (valid[u]) add_into(seg, val[u]);
+            }
+        }
+        add_into(acc, seg);
+        st_pack(state + row * a.ld_state + c, acc);
+    }
+}
+
+constexpr int kWideThreads = 128;
+
+template <typename T, int V, int INIT, bool EXACT>
+__global__ void __launch_bounds__(kWideThreads) level_wide_kernel(LevelArgs a) {
+    __shared__ Pack<T, V> red[kWideThreads];
+    __shared__ uint32_t codes[kWideThreads];
+    const int64_t local = __ldg(a.heavy_rows + blockIdx.x);
+    const int32_t e0 = __ldg(a.row_ptr + local);
+    const int32_t e1 = __ldg(a.row_ptr + local + 1);
+    const int64_t row = a.row_begin + local;
+    const int g_lanes = 1 << a.log2g;                // lanes per column group
+    const int groups = kWideThreads >> a.log2g;      // entry groups
+    const int lane = threadIdx.x & (g_lanes - 1);
+    const int grp = threadIdx.x >> a.log2g;
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t base = 0; base < a.k; base += step) {  // uniform trip count across the CTA
+        const int64_t c = base + static_cast<int64_t>(lane) * V;
+        const bool active = c < a.k;
+        if constexpr (!EXACT) {
+            Pack<T, V> part = zero_pack<T, V>();
+            if (active) {
+                for (int32_t e = e0 + grp; e < e1; e += groups) {
+                    const T* src = entry_row<T>(a, __ldg(a.entries + e));
+                    if (src) add_into(part, ld_ro<T, V>(src + c));
+                }
+            }
+            red[threadIdx.x] = part;
+            __syncthreads();
+            for (int s = groups >> 1; s > 0; s >>= 1) {
+                if (grp < s) {
+                    Pack<T, V> other = red[threadIdx.x + (s << a.log2g)];
+                    add_into(red[threadIdx.x], other);
+                }
+                __syncthreads();
+            }
+            if (grp == 0 && active) {
+                Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+                add_into(acc, red[threadIdx.x]);
+                st_pack(state + row * a.ld_state + c, acc);
+            }
+            __syncthreads();
+        } else {
+            Pack<T, V> acc = zero_pack<T, V>();
+            Pack<T, V> seg = zero_pack<T, V>();
+            if (grp == 0 && active) acc = init_value<T, V, INIT>(a, row, c);
+            for (int32_t s0 = e0; s0 < e1; s0 += groups) {
+                const int32_t e = s0 + grp;
+                Pack<T, V> val = zero_pack<T, V>();
+                uint32_t code = 0;
+                if (e < e1) {
+                    code = __ldg(a.entries + e);
+                    const T* src = entry_row<T>(a, code);
+                    if (src && active) val = ld_ro<T, V>(src + c);
+                }
+                red[threadIdx.x] = val;
+                if (lane == 0) codes[grp] = code;
+                __syncthreads();
+                if (grp == 0 && active) {
+                    const int n = min(groups, e1 - s0);
+                    for (int i = 0; i < n; ++i) {
+                        if (codes[i] & GRG_B200_SEG_START) {
+                            add_into(acc, seg);
+                            seg = zero_pack<T, V>();
+                        }
+                        add_into(seg, red[(i << a.log2g) + lane]);
+                    }
+                }
+                __syncthreads();
+            }
+            if (grp == 0 && active) {
+                add_into(acc, seg);
+                st_pack(state + row * a.ld_state + c, acc);
+            }
+        }
+    }
+}
+
+// Up seeding of level 0: state[r] = init(r) (+ input row for samples).
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(256) seed_up_kernel(LevelArgs a, int64_t num_samples, const int32_t* s2i, int32_t by_ind) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t row = t >> a.log2g;
+    if (row >= a.num_rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    T* state = static_cast<T*>(a.state);
+    int64_t xrow = row;
+    if (row < num_samples && by_ind) {
+        xrow = __ldg(s2i + row);
+        if (a.err && (xrow < 0 || xrow >= a.lim_x)) {
+            report(a.err, kErrInputId);
+            return;
+        }
+    }
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step) {
+        Pack<T, V> v = init_value<T, V, INIT>(a, row, c);
+        if (row < num_samples) add_into(v, ld_ro<T, V>(static_cast<const T*>(a.x) + xrow * a.ld_x + c));
+        st_pack(state + row * a.ld_state + c, v);
+    }
+}
+
+struct OutArgs {
+    int64_t rows;
+    const int32_t* ptr;    // selector / individual CSR
+    const int32_t* idx;
+    const void* state;
+    int64_t ld_state;
+    void* out;
+    int64_t ld_out;
+    const void* bias;      // per output row (up) or per sample (down)
+    const void* init_vector;
+    int32_t bias_mode;
+    int64_t k;
+    int32_t log2g;
+    int32_t* err;
+    int64_t lim;
+};
+
+template <typename T, int V>
+__device__ __forceinline__ void apply_bias(const OutArgs& a, int64_t r, int64_t c, Pack<T, V>& v) {
+    if (a.bias_mode == GRG_B200_BIAS_XTX) {
+        const T b = __ldg(static_cast<const T*>(a.bias) + r);
+#pragma unroll
+        for (int i = 0; i < V; ++i) v.v[i] = add_rn(v.v[i], b);
+    } else if (a.bias_mode == GRG_B200_BIAS_VECTOR) {
+        const T b = __ldg(static_cast<const T*>(a.bias) + r);
+        const Pack<T, V> iv = ld_ro<T, V>(static_cast<const T*>(a.init_vector) + c);
+#pragma unroll
+        for (int i = 0; i < V; ++i) v.v[i] = add_rn(v.v[i], mul_rn(b, iv.v[i]));
+    }
+}
+
+// out[r] = sum over idx[ptr[r]..ptr[r+1]) of state rows (from zero, in order) + bias.
+template <typename T, int V, bool BIAS_PER_ENTRY>
+__global__ void __launch_bounds__(256) gather_out_kernel(OutArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t r = t >> a.log2g;
+    if (r >= a.rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    const int32_t e0 = __ldg(a.ptr + r), e1 = __ldg(a.ptr + r + 1);
+    const T* state = static_cast<const T*>(a.state);
+    T* out = static_cast<T*>(a.out);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step) {
+        Pack<T, V> s = zero_pack<T, V>();
+        for (int32_t e = e0; e < e1; ++e) {
+            const int64_t n = __ldg(a.idx + e);
+            if (a.err && (n < 0 || n >= a.lim)) {
+                report(a.err, kErrSelector);
+                continue;
+            }
+            Pack<T, V> v = ld_ro<T, V>(state + n * a.ld_state + c);
+            if constexpr (BIAS_PER_ENTRY) apply_bias<T, V>(a, n, c, v);  // down by individual
+            add_into(s, v);
+        }
+        if constexpr (!BIAS_PER_ENTRY) apply_bias<T, V>(a, r, c, s);
+        st_pack(out + r * a.ld_out + c, s);
+    }
+}
+
+// Down output without grouping: out[s] = state[s] + bias[s].
+template <typename T, int V>
+__global__ void __launch_bounds__(256) copy_out_kernel(OutArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t r = t >> a.log2g;
+    if (r >= a.rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    const T* state = static_cast<const T*>(a.state);
+    T* out = static_cast<T*>(a.out);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step) {
+        Pack<T, V> v = ld_ro<T, V>(state + r * a.ld_state + c);
+        apply_bias<T, V>(a, r, c, v);
+        st_pack(out + r * a.ld_out + c, v);
+    }
+}
+
+// All nodes in original order: out[j] = state[inv_perm[j]].
+template <typename T, int V>
+__global__ void __launch_bounds__(256) emit_all_kernel(OutArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t j = t >> a.log2g;
+    if (j >= a.rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    const int64_t n = __ldg(a.idx + j);
+    if (a.err && (n < 0 || n >= a.lim)) {
+        report(a.err, kErrPerm);
+        return;
+    }
+    const T* state = static_cast<const T*>(a.state);
+    T* out = static_cast<T*>(a.out);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step)
+        st_pack(out + j * a.ld_out + c, ld_ro<T, V>(state + n * a.ld_state + c));
+}
+
+// ---------------------------------------------------------------------------------------
+// Host-side launch helpers
+// ---------------------------------------------------------------------------------------
+struct Shape {
+    int vec;    // V
+    int log2g;  // lanes per row = 1 << log2g
+};
+
+bool aligned(const void* p, int bytes) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
+
+Shape choose_shape(const grg_b200_traverse_args* a) {
+    const int esize = a->dtype == GRG_B200_F64 ? 8 : 4;
+    const int64_t lds[] = {a->ld_state, a->ld_input, a->ld_output, a->use_miss ? a->ld_miss : 0, a->ld_init};
+    const void* ptrs[] = {a->state, a->input, a->output, a->use_miss ? a->miss : nullptr, a->init_vector, a->init_matrix};
+    int vec = 1;
+    const int candidates[] = {4, 2};
+    for (int v : candidates) {
+        if (a->dtype == GRG_B200_F64 && v == 4) continue;
+        bool ok = a->k % v == 0;
+        for (int64_t ld : lds) ok = ok && (ld % v == 0);
+        for (const void* p : ptrs) ok = ok && aligned(p, v * esize);
+        if (ok) {
+            vec = v;
+            break;
+        }
+    }
+    const int64_t cols = (a->k + vec - 1) / vec;
+    int log2g = 0;
+    while ((1 << log2g) < cols && log2g < 5) ++log2g;
+    return {vec, log2g};
+}
+
+dim3 grid_for(int64_t rows, int log2g, int threads) {
+    const int64_t total = rows << log2g;
+    return dim3(static_cast<unsigned>((total + threads - 1) / threads));
+}
+
+int validate_common(const grg_b200_traverse_args* a) {
+    if (!a) return fail(GRG_B200_ERR_INVALID, "args is NULL");
+    if (a->dtype != GRG_B200_F64 && a->dtype != GRG_B200_F32) return fail(GRG_B200_ERR_INVALID, "unknown dtype %d", a->dtype);
+    if (a->k < 1) return fail(GRG_B200_ERR_INVALID, "k must be >= 1, got %lld", (long long)a->k);
+    if (a->ld_state < a->k) return fail(GRG_B200_ERR_INVALID, "ld_state %lld < k %lld", (long long)a->ld_state, (long long)a->k);
+    if (!a->state) return fail(GRG_B200_ERR_INVALID, "state is NULL");
+    if (a->num_nodes > (int64_t)GRG_B200_MAX_ID + 1 || a->num_mutations > (int64_t)GRG_B200_MAX_ID + 1)
+        return fail(GRG_B200_ERR_UNSUPPORTED, "node/mutation counts above %u are not supported", GRG_B200_MAX_ID + 1u);
+    if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
+    if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
+    if (a->init_mode == GRG_B200_INIT_XTX && !a->xtx_node) return fail(GRG_B200_ERR_INVALID, "xtx_node is NULL");
+    if (a->init_mode == GRG_B200_INIT_MATRIX && (!a->init_matrix || !a->node_perm || a->ld_init < a->k))
+        return fail(GRG_B200_ERR_INVALID, "init_matrix/node_perm missing or ld_init < k");
+    if (a->bias_mode < 0 || a->bias_mode > 2) return fail(GRG_B200_ERR_INVALID, "unknown bias_mode %d", a->bias_mode);
+    if (a->bias_mode != GRG_B200_BIAS_NONE && !a->endpoint_bias) return fail(GRG_B200_ERR_INVALID, "endpoint_bias is NULL");
+    if (a->bias_mode == GRG_B200_BIAS_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
+    return GRG_B200_OK;
+}
+
+LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
+    LevelArgs la{};
+    la.use_miss = a->direction == GRG_B200_DOWN && a->use_miss;
+    la.state = a->state;
+    la.ld_state = a->ld_state;
+    la.x = a->input;
+    la.ld_x = a->ld_input;
+    la.miss = a->miss;
+    la.ld_miss = a->ld_miss;
+    la.init_vector = a->init_vector;
+    la.init_matrix = a->init_matrix;
+    la.ld_init = a->ld_init;
+    la.node_perm = a->node_perm;
+    la.xtx_node = a->xtx_node;
+    la.k = a->k;
+    la.log2g = sh.log2g;
+    la.err = a->error_word;
+    la.lim_state = a->num_nodes;
+    la.lim_x = a->direction == GRG_B200_UP ? (a->by_individual ? a->num_individuals : a->num_samples) : a->num_mutations;
+    la.lim_miss = a->num_mutations;
+    return la;
+}
+
+template <typename T, int V>
+int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, cudaStream_t s) {
+    if (la.num_rows > 0) {
+        const dim3 grid = grid_for(la.num_rows, la.log2g, 256);
+        switch (init_mode) {
+            case 0: level_narrow_kernel<T, V, 0><<<grid, 256, 0, s>>>(la); break;
+            case 1: level_narrow_kernel<T, V, 1><<<grid, 256, 0, s>>>(la); break;
+            case 2: level_narrow_kernel<T, V, 2><<<grid, 256, 0, s>>>(la); break;
+            default: level_narrow_kernel<T, V, 3><<<grid, 256, 0, s>>>(la); break;
+        }
+        GRG_LAUNCH_CHECK("level_narrow_kernel");
+    }
+    if (la.num_heavy > 0) {
+        const dim3 grid(static_cast<unsigned>(la.num_heavy));
+#define GRG_WIDE(INIT)                                                                            \
+    if (exact) level_wide_kernel<T, V, INIT, true><<<grid, kWideThreads, 0, s>>>(la);            \
+    else level_wide_kernel<T, V, INIT, false><<<grid, kWideThreads, 0, s>>>(la);
+        switch (init_mode) {
+            case 0: GRG_WIDE(0) break;
+            case 1: GRG_WIDE(1) break;
+            case 2: GRG_WIDE(2) break;
+            default: GRG_WIDE(3) break;
+        }
+#undef GRG_WIDE
+        GRG_LAUNCH_CHECK("level_wide_kernel");
+    }
+    return GRG_B200_OK;
+}
+
+template <typename F>
+int dispatch(const grg_b200_traverse_args* a, const Shape& sh, F&& f) {
+    if (a->dtype == GRG_B200_F64) {
+        if (sh.vec == 2) return f(double{}, std::integral_constant<int, 2>{});
+        return f(double{}, std::integral_constant<int, 1>{});
+    }
+    if (sh.vec == 4) return f(float{}, std::integral_constant<int, 4>{});
+    if (sh.vec == 2) return f(float{}, std::integral_constant<int, 2>{});
+    return f(float{}, std::integral_constant<int, 1>{});
+}
+
+int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level* L, const void* blob, cudaStream_t s) {
+    if (L->num_rows < 0 || L->num_heavy < 0 || L->num_entries < 0)
+        return fail(GRG_B200_ERR_INVALID, "negative level sizes");
+    if (L->num_rows == 0) return GRG_B200_OK;
+    if (!blob) return fail(GRG_B200_ERR_INVALID, "level blob is NULL");
+    if (L->row_begin < 0 || L->row_begin + L->num_rows > a->num_nodes)
+        return fail(GRG_B200_ERR_INVALID, "level rows [%lld, %lld) outside the %lld nodes", (long long)L->row_begin,
+                    (long long)(L->row_begin + L->num_rows), (long long)a->num_nodes);
+    const char* base = static_cast<const char*>(blob);
+    LevelArgs la = level_args(a, sh);
+    la.row_begin = L->row_begin;
+    la.num_rows = L->num_rows;
+    la.row_ptr = reinterpret_cast<const int32_t*>(base + L->off_row_ptr);
+    la.entries = reinterpret_cast<const uint32_t*>(base + L->off_entries);
+    la.heavy_rows = reinterpret_cast<const int32_t*>(base + L->off_heavy);
+    la.num_heavy = L->num_heavy;
+    la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
+    const bool exact = a->exact_order != 0;
+    return dispatch(a, sh, [&](auto t, auto v) {
+        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, s);
+    });
+}
+
+int seed_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    if (a->level0_rows <= 0) return GRG_B200_OK;
+    if (!a->input) return fail(GRG_B200_ERR_INVALID, "input is NULL");
+    if (a->by_individual && !a->sample_to_individual) return fail(GRG_B200_ERR_INVALID, "sample_to_individual is NULL");
+    LevelArgs la = level_args(a, sh);
+    la.row_begin = 0;
+    la.num_rows = a->level0_rows;
+    const dim3 grid = grid_for(la.num_rows, la.log2g, 256);
+    return dispatch(a, sh, [&](auto t, auto v) {
+        using T = decltype(t);
+        constexpr int V = decltype(v)::value;
+        switch (a->init_mode) {
+            case 0: seed_up_kernel<T, V, 0><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            case 1: seed_up_kernel<T, V, 1><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            case 2: seed_up_kernel<T, V, 2><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            default: seed_up_kernel<T, V, 3><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+        }
+        GRG_LAUNCH_CHECK("seed_up_kernel");
+        return (int)GRG_B200_OK;
+    });
+}
+
+OutArgs out_args(const grg_b200_traverse_args* a, const Shape& sh) {
+    OutArgs o{};
+    o.state = a->state;
+    o.ld_state = a->ld_state;
+    o.out = a->output;
+    o.ld_out = a->ld_output;
+    o.bias = a->endpoint_bias;
+    o.init_vector = a->init_vector;
+    o.bias_mode = a->emit_all_nodes ? GRG_B200_BIAS_NONE : a->bias_mode;
+    o.k = a->k;
+    o.log2g = sh.log2g;
+    o.err = a->error_word;
+    o.lim = a->num_nodes;
+    return o;
+}
+
+int output_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    if (!a->output || !a->sel_mut_ptr || (!a->sel_mut_idx && a->num_mutations > 0))
+        return fail(GRG_B200_ERR_INVALID, "up output needs output and sel_mut");
+    if (a->use_miss && (!a->miss || !a->sel_miss_ptr)) return fail(GRG_B200_ERR_INVALID, "up miss output needs miss and sel_miss");
+    if (a->num_mutations == 0) return GRG_B200_OK;
+    OutArgs o = out_args(a, sh);
+    o.rows = a->num_mutations;
+    o.ptr = a->sel_mut_ptr;
+    o.idx = a->sel_mut_idx;
+    const dim3 grid = grid_for(o.rows, o.log2g, 256);
+    return dispatch(a, sh, [&](auto t, auto v) {
+        using T = decltype(t);
+        constexpr int V = decltype(v)::value;
+        gather_out_kernel<T, V, false><<<grid, 256, 0, s>>>(o);
+        GRG_LAUNCH_CHECK("gather_out_kernel(sel_mut)");
+        if (a->use_miss) {
+            OutArgs m = o;
+            m.ptr = a->sel_miss_ptr;
+            m.idx = a->sel_miss_idx;
+            m.out = a->miss;
+            m.ld_out = a->ld_miss;
+            m.bias_mode = GRG_B200_BIAS_NONE;
+            gather_out_kernel<T, V, false><<<grid, 256, 0, s>>>(m);
+            GRG_LAUNCH_CHECK("gather_out_kernel(sel_miss)");
+        }
+        return (int)GRG_B200_OK;
+    });
+}
+
+int output_down_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    if (!a->output) return fail(GRG_B200_ERR_INVALID, "output is NULL");
+    OutArgs o = out_args(a, sh);
+    if (a->by_individual) {
+        if (!a->ind_ptr || !a->ind_samples) return fail(GRG_B200_ERR_INVALID, "by_individual needs ind_ptr/ind_samples");
+        o.rows = a->num_individuals;
+        o.ptr = a->ind_ptr;
+        o.idx = a->ind_samples;
+        o.lim = a->num_samples;
+    } else {
+        o.rows = a->num_samples;
+    }
+    if (o.rows == 0) return GRG_B200_OK;
+    const dim3 grid = grid_for(o.rows, o.log2g, 256);
+    return dispatch(a, sh, [&](auto t, auto v) {
+        using T = decltype(t);
+        constexpr int V = decltype(v)::value;
+        if (a->by_individual) gather_out_kernel<T, V, true><<<grid, 256, 0, s>>>(o);
+        else copy_out_kernel<T, V><<<grid, 256, 0, s>>>(o);
+        GRG_LAUNCH_CHECK("output_down");
+        return (int)GRG_B200_OK;
+    });
+}
+
+int emit_all_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    if (!a->output || !a->inv_node_perm) return fail(GRG_B200_ERR_INVALID, "emit_all_nodes needs output and inv_node_perm");
+    OutArgs o = out_args(a, sh);
+    o.rows = a->num_nodes;
+    o.idx = a->inv_node_perm;
+    const dim3 grid = grid_for(o.rows, o.log2g, 256);
+    return dispatch(a, sh, [&](auto t, auto v) {
+        using T = decltype(t);
+        constexpr int V = decltype(v)::value;
+        emit_all_kernel<T, V><<<grid, 256, 0, s>>>(o);
+        GRG_LAUNCH_CHECK("emit_all_kernel");
+        return (int)GRG_B200_OK;
+    });
+}
+
+}  // namespace
+
+struct grg_b200_ring {
+    int device;
+    int num_slots;
+    cudaStream_t copy;
+    cudaEvent_t fork;
+    cudaEvent_t join;
+    cudaEvent_t* ready;
+    cudaEvent_t* free_ev;
+};
+
+extern "C" {
+
+int grg_b200_abi_version(void) { return GRG_B200_ABI_VERSION; }
+
+size_t grg_b200_last_error(char* buf, size_t buf_size) {
+    const size_t n = strlen(g_last_error);
+    if (buf && buf_size) {
+        const size_t m = n < buf_size - 1 ? n : buf_size - 1;
+        memcpy(buf, g_last_error, m);
+        buf[m] = '\0';
+    }
+    return n;
+}
+
+int grg_b200_ring_create(int device, int num_slots, grg_b200_ring** out) {
+    if (!out || num_slots < 1) return fail(GRG_B200_ERR_INVALID, "ring needs num_slots >= 1 and an out pointer");
+    *out = nullptr;
+    int prev = 0;
+    GRG_CUDA_TRY(cudaGetDevice(&prev));
+    GRG_CUDA_TRY(cudaSetDevice(device));
+    grg_b200_ring* r = new grg_b200_ring{};
+    r->device = device;
+    r->num_slots = num_slots;
+    r->ready = new cudaEvent_t[num_slots]();
+    r->free_ev = new cudaEvent_t[num_slots]();
+    cudaError_t e = cudaStreamCreateWithFlags(&r->copy, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->join, cudaEventDisableTiming);
+    for (int i = 0; i < num_slots && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&r->ready[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&r->free_ev[i], cudaEventDisableTiming);
+    }
+    cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        grg_b200_ring_destroy(r);
+        return fail(GRG_B200_ERR_CUDA, "ring creation failed: %s", cudaGetErrorString(e));
+    }
+    *out = r;
+    return GRG_B200_OK;
+}
+
+int grg_b200_ring_destroy(grg_b200_ring* r) {
+    if (!r) return GRG_B200_OK;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(r->device);
+    if (r->copy) cudaStreamSynchronize(r->copy);
+    for (int i = 0; i < r->num_slots; ++i) {
+        if (r->ready && r->ready[i]) cudaEventDestroy(r->ready[i]);
+        if (r->free_ev && r->free_ev[i]) cudaEventDestroy(r->free_ev[i]);
+    }
+    if (r->fork) cudaEventDestroy(r->fork);
+    if (r->join) cudaEventDestroy(r->join);
+    if (r->copy) cudaStreamDestroy(r->copy);
+    cudaSetDevice(prev);
+    delete[] r->ready;
+    delete[] r->free_ev;
+    delete r;
+    return GRG_B200_OK;
+}
+
+int grg_b200_seed_up(const grg_b200_traverse_args* a, void* stream) {
+    int rc = validate_common(a);
+    if (rc) return rc;
+    return seed_up_impl(a, choose_shape(a), static_cast<cudaStream_t>(stream));
+}
+
+int grg_b200_run_level(const grg_b200_traverse_args* a, const grg_b200_level* level, void* stream) {
+    int rc = validate_common(a);
+    if (rc) return rc;
+    if (!level) return fail(GRG_B200_ERR_INVALID, "level is NULL");
+    return run_level(a, choose_shape(a), level, level->blob, static_cast<cudaStream_t>(stream));
+}
+
+int grg_b200_output_up(const grg_b200_traverse_args* a, void* stream) {
+    int rc = validate_common(a);
+    if (rc) return rc;
+    return output_up_impl(a, choose_shape(a), static_cast<cudaStream_t>(stream));
+}
+
+int grg_b200_output_down(const grg_b200_traverse_args* a, void* stream) {
+    int rc = validate_common(a);
+    if (rc) return rc;
+    return output_down_impl(a, choose_shape(a), static_cast<cudaStream_t>(stream));
+}
+
+int grg_b200_emit_all(const grg_b200_traverse_args* a, void* stream) {
+    int rc = validate_common(a);
+    if (rc) return rc;
+    return emit_all_impl(a, choose_shape(a), static_cast<cudaStream_t>(stream));
+}
+
+int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
+    int rc = validate_common(a);
+    if (rc) return rc;
+    if (a->num_levels < 0 || (a->num_levels > 0 && !a->levels)) return fail(GRG_B200_ERR_INVALID, "levels missing");
+    if (a->direction == GRG_B200_DOWN && !a->input && a->num_mutations > 0) return fail(GRG_B200_ERR_INVALID, "input is NULL");
+    if (a->direction == GRG_B200_DOWN && a->use_miss && !a->miss) return fail(GRG_B200_ERR_INVALID, "miss input is NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+    const Shape sh = choose_shape(a);
+
+    bool any_streamed = false;
+    for (int i = 0; i < a->num_levels; ++i) {
+        const grg_b200_level& L = a->levels[i];
+        if (L.slot >= 0) {
+            any_streamed = true;
+            if (!a->ring || L.slot >= a->num_slots || L.slot >= a->ring->num_slots || !a->slot_buffers || !a->slot_bytes)
+                return fail(GRG_B200_ERR_INVALID, "level %d is streamed through slot %d but the ring is missing or too small", i, L.slot);
+            if (L.blob_bytes > a->slot_bytes[L.slot])
+                return fail(GRG_B200_ERR_INVALID, "level %d needs %lld bytes, slot %d has %lld", i, (long long)L.blob_bytes,
+                            L.slot, (long long)a->slot_bytes[L.slot]);
+        }
+    }
+
+    if (a->direction == GRG_B200_UP) {
+        rc = seed_up_impl(a, sh, s);
+        if (rc) return rc;
+    }
+    // Fork the copy stream off the caller's stream so streamed copies are ordered after the
+    // caller's earlier work (and join a CUDA graph capture in progress).
+    bool used[256] = {false};
+    if (any_streamed) {
+        if (a->ring->num_slots > 256) return fail(GRG_B200_ERR_UNSUPPORTED, "at most 256 ring slots");
+        GRG_CUDA_TRY(cudaEventRecord(a->ring->fork, s));
+        GRG_CUDA_TRY(cudaStreamWaitEvent(a->ring->copy, a->ring->fork, 0));
+    }
+    for (int i = 0; i < a->num_levels; ++i) {
+        const grg_b200_level& L = a->levels[i];
+        const void* blob = L.blob;
+        if (L.slot >= 0 && L.num_rows > 0) {
+            grg_b200_ring* r = a->ring;
+            if (used[L.slot]) GRG_CUDA_TRY(cudaStreamWaitEvent(r->copy, r->free_ev[L.slot], 0));
+            GRG_CUDA_TRY(cudaMemcpyAsync(a->slot_buffers[L.slot], L.blob, static_cast<size_t>(L.blob_bytes), cudaMemcpyHostToDevice, r->copy));
+            GRG_CUDA_TRY(cudaEventRecord(r->ready[L.slot], r->copy));
+            GRG_CUDA_TRY(cudaStreamWaitEvent(s, r->ready[L.slot], 0));
+            blob = a->slot_buffers[L.slot];
+        }
+        rc = run_level(a, sh, &L, blob, s);
+        if (rc) return rc;
+        if (L.slot >= 0 && L.num_rows > 0) {
+            GRG_CUDA_TRY(cudaEventRecord(a->ring->free_ev[L.slot], s));
+            used[L.slot] = true;
+        }
+    }
+    if (any_streamed) {
+        GRG_CUDA_TRY(cudaEventRecord(a->ring->join, a->ring->copy));
+        GRG_CUDA_TRY(cudaStreamWaitEvent(s, a->ring->join, 0));
+    }
+    if (a->emit_all_nodes) return emit_all_impl(a, sh, s);
+    if (a->direction == GRG_B200_UP) return output_up_impl(a, sh, s);
+    return output_down_impl(a, sh, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+/*
+ * grg_b200.h - C ABI of the B200 GRG matmul backend (libgrg_b200.so).
+ *
+ * The library computes the GRG "up" (X*G, samples -> mutations) and "down" (X*G^T,
+ * mutations -> samples) traversals on one NVIDIA B200 (sm_100a).  All entry points take
+ * plain device/host pointers, sizes and a cudaStream_t; none allocates device memory: the
+ * caller (the Python runtime, via PyTorch) owns every buffer.  Every function returns a
+ * grg_b200_status; grg_b200_last_error() gives the message of the last failure on the
+ * calling thread.  Launches are asynchronous on the given stream and may be captured in a
+ * CUDA graph.
+ *
+ * Replaced reference interfaces (paths inside CornellHPC/grg-spmv):
+ *   grg_b200_traverse      - the whole prepared call: TritonRuntime._execute_prepared
+ *                            (pygrgl_spmv/backends/triton/backend.py:1221-1225), i.e.
+ *                            _seed_state (:1116-1150), _enqueue_wavefront (:970-1049) with
+ *                            launch_block / csr_spmm_add_kernel / csc_spmm_add_kernel
+ *                            (pygrgl_spmv/backends/triton/kernel.py:57-206), and
+ *                            _write_output (:1178-1219) with _apply_endpoint_bias (:1152-1176);
+ *                            the cuSPARSE equivalent is CusparseRuntime._seed_prepared,
+ *                            _enqueue_wavefront, _write_prepared_output
+ *                            (pygrgl_spmv/backends/cusparse/backend.py:1633-1828).
+ *   grg_b200_seed_up       - the up branch of _seed_state (triton/backend.py:1120-1141).
+ *   grg_b200_run_level     - one destination level of _enqueue_wavefront: every
+ *                            launch_block call of that level fused into one gather pass
+ *                            (triton/backend.py:1030-1046); for down it also performs the
+ *                            selector scatter of _seed_state (:1143-1150) as a gather.
+ *   grg_b200_output_up     - the up branch of _write_output (triton/backend.py:1189-1210).
+ *   grg_b200_output_down   - the down branch of _write_output (triton/backend.py:1212-1219).
+ *   grg_b200_emit_all      - the emit_all_nodes branch of _write_output (:1185-1187).
+ *   grg_b200_ring_create / grg_b200_ring_destroy
+ *                          - the per-slot copy streams and events of the streamed ring
+ *                            (triton/backend.py:710, :738-746, :958-968).
+ *   grg_b200_last_error    - error reporting (the Python side raises RuntimeError with it).
+ *
+ * Data layout (all ids are positions in the artifact's stable height order):
+ *   state   [num_nodes, ld_state]     node values, row-major
+ *   input   [rows, ld_input]          up: samples (or individuals), down: mutations
+ *   output  [rows, ld_output]         up: mutations, down: samples (or individuals),
+ *                                     emit_all_nodes: all nodes in ORIGINAL node order
+ *   level   a gather list per destination row: the row's value is
+ *             init(row) + seg_1 + seg_2 + ...   (left to right)
+ *           where each segment is a sum, from zero and in list order, of the entries that
+ *           follow a GRG_B200_SEG_START-flagged entry.  An entry names a state row, an
+ *           input row or a miss row (GRG_B200_SRC_*).  This reproduces the accumulation
+ *           order of the reference's ReferenceRuntime (per source level, one sparse product
+ *           added to the destination; pygrgl_spmv/backends/reference.py:396-429).
+ */
+#ifndef GRG_B200_H
+#define GRG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GRG_B200_ABI_VERSION 1
+
+typedef enum grg_b200_status {
+    GRG_B200_OK = 0,
+    GRG_B200_ERR_INVALID = 1,     /* bad argument; nothing was launched */
+    GRG_B200_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    GRG_B200_ERR_UNSUPPORTED = 3  /* valid request outside this build's limits */
+} grg_b200_status;
+
+typedef enum grg_b200_dtype { GRG_B200_F64 = 0, GRG_B200_F32 = 1 } grg_b200_dtype;
+typedef enum grg_b200_direction { GRG_B200_UP = 0, GRG_B200_DOWN = 1 } grg_b200_direction;
+typedef enum grg_b200_init {
+    GRG_B200_INIT_NONE = 0,
+    GRG_B200_INIT_VECTOR = 1,  /* every node starts at init_vector[col] */
+    GRG_B200_INIT_XTX = 2,     /* every node starts at xtx_node[row] (2 * coalescence count) */
+    GRG_B200_INIT_MATRIX = 3   /* node row starts at init_matrix[node_perm[row], col] */
+} grg_b200_init;
+typedef enum grg_b200_bias {
+    GRG_B200_BIAS_NONE = 0,
+    GRG_B200_BIAS_VECTOR = 1,  /* out[r, c] += bias[r] * init_vector[c] (product rounded first) */
+    GRG_B200_BIAS_XTX = 2      /* out[r, c] += bias[r] */
+} grg_b200_bias;
+
+/* Gather-list entry coding (uint32). */
+#define GRG_B200_SEG_START 0x80000000u
+#define GRG_B200_SRC_SHIFT 29
+#define GRG_B200_SRC_MASK 0x3u
+#define GRG_B200_SRC_STATE 0u /* id = state row */
+#define GRG_B200_SRC_INPUT 1u /* id = input row (down: mutation) */
+#define GRG_B200_SRC_MISS 2u  /* id = miss row (down: mutation), skipped unless use_miss */
+#define GRG_B200_ID_MASK 0x1FFFFFFFu
+#define GRG_B200_MAX_ID 0x1FFFFFFFu
+
+/*
+ * One destination level.  Its gather structure is one byte blob with three arrays at
+ * 16-byte aligned offsets:
+ *   int32  row_ptr[num_rows + 1]     entry offsets of each row
+ *   int32  heavy_rows[num_heavy]     level-local rows with more than heavy_threshold
+ *                                    entries (processed one CTA per row)
+ *   uint32 entries[num_entries]
+ * slot < 0: blob is device memory.  slot >= 0: blob is pinned host memory that
+ * grg_b200_traverse copies into ring slot `slot` before the level runs.
+ */
+typedef struct grg_b200_level {
+    int64_t row_begin;
+    int64_t num_rows;
+    int64_t num_entries;
+    int64_t num_heavy;
+    int32_t heavy_threshold;
+    int32_t slot;
+    const void* blob;
+    int64_t blob_bytes;
+    int64_t off_row_ptr;
+    int64_t off_heavy;
+    int64_t off_entries;
+} grg_b200_level;
+
+typedef struct grg_b200_ring grg_b200_ring; /* opaque: copy stream + per-slot events */
+
+typedef struct grg_b200_traverse_args {
+    int32_t dtype;        /* grg_b200_dtype */
+    int32_t direction;    /* grg_b200_direction */
+    int32_t init_mode;    /* grg_b200_init (applied inside the traversal) */
+    int32_t bias_mode;    /* grg_b200_bias (applied to the output) */
+    int32_t emit_all_nodes;
+    int32_t by_individual;
+    int32_t use_miss;     /* down: read miss rows; up: write miss output */
+    int32_t exact_order;  /* 1: heavy rows also sum in list order (bit-exact with the reference) */
+    int64_t k;
+    int64_t num_nodes;
+    int64_t num_samples;
+    int64_t num_mutations;
+    int64_t num_individuals;
+    void* state;
+    int64_t ld_state;
+    const void* input;
+    int64_t ld_input;
+    void* output;
+    int64_t ld_output;
+    void* miss; /* down: miss input [M, ld_miss]; up: miss output [M, ld_miss] */
+    int64_t ld_miss;
+    const void* init_vector;            /* [k] */
+    const void* init_matrix;            /* [num_nodes, ld_init], original node order */
+    int64_t ld_init;
+    const int32_t* node_perm;           /* [num_nodes] stable position -> original id */
+    const int32_t* inv_node_perm;       /* [num_nodes] original id -> stable position */
+    const void* xtx_node;               /* [num_nodes] 2 * coalescence count, stable order */
+    const void* endpoint_bias;          /* up: [num_mutations], down: [num_samples] */
+    const int32_t* sample_to_individual;/* up by_individual: [num_samples] */
+    const int32_t* ind_ptr;             /* down by_individual: [num_individuals + 1] */
+    const int32_t* ind_samples;         /* down by_individual: samples of each individual, ascending */
+    const int32_t* sel_mut_ptr;         /* up: [num_mutations + 1] */
+    const int32_t* sel_mut_idx;         /* up: node of each selector entry, stored order */
+    const int32_t* sel_miss_ptr;
+    const int32_t* sel_miss_idx;
+    int64_t level0_rows;                /* up: number of level-0 rows to seed */
+    int32_t num_levels;                 /* levels in execution order */
+    const grg_b200_level* levels;
+    grg_b200_ring* ring;                /* required when any level is streamed */
+    void* const* slot_buffers;          /* device ring slots */
+    const int64_t* slot_bytes;
+    int32_t num_slots;
+    int32_t* error_word;                /* optional device int32: first failed bounds check */
+} grg_b200_traverse_args;
+
+/* Library ABI version (GRG_B200_ABI_VERSION of the build). */
+int grg_b200_abi_version(void);
+
+/* Copies the last error message of the calling thread into buf (always NUL-terminated). */
+size_t grg_b200_last_error(char* buf, size_t buf_size);
+
+/* Ring of streamed-structure slots: one non-blocking copy stream on `device` and two events
+ * per slot.  Replaces the Triton runtime's slot copy streams and copy/compute events. */
+int grg_b200_ring_create(int device, int num_slots, grg_b200_ring** out);
+int grg_b200_ring_destroy(grg_b200_ring* ring);
+
+/* Seeds level 0 of an up traversal: state[r] = init(r) (+ input[r or sample_to_individual[r]]
+ * for r < num_samples).  Uses dtype, init_mode, by_individual, k, the state/input/init fields
+ * and level0_rows of args. */
+int grg_b200_seed_up(const grg_b200_traverse_args* args, void* stream);
+
+/* Runs one destination level (narrow rows, then heavy rows).  The level's blob must already
+ * be device-resident (slot < 0) or copied (blob then names the device copy). */
+int grg_b200_run_level(const grg_b200_traverse_args* args, const grg_b200_level* level, void* stream);
+
+/* Up outputs: output[m] = sum of state rows of sel_mut row m (stored order) + endpoint bias;
+ * with use_miss also miss[m] from sel_miss (no bias). */
+int grg_b200_output_up(const grg_b200_traverse_args* args, void* stream);
+
+/* Down output: output[s] = state[s] + bias[s], or with by_individual
+ * output[i] = sum over the individual's samples (ascending) of (state[s] + bias[s]). */
+int grg_b200_output_down(const grg_b200_traverse_args* args, void* stream);
+
+/* All-node output in original order: output[j] = state[inv_node_perm[j]]. */
+int grg_b200_emit_all(const grg_b200_traverse_args* args, void* stream);
+
+/* The full prepared call: seed, every level (copying streamed levels through the ring), and
+ * the output stage, all on `stream`. */
+int grg_b200_traverse(const grg_b200_traverse_args* args, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRG_B200_H */

@@ -1,0 +1,90 @@
+"""B200 runtime vs the reference: golden vectors (bit-exact) and the oracle on larger graphs."""
+
+from __future__ import annotations
+
+from contextlib import ExitStack
+
+import numpy as np
+import pytest
+
+from conftest import ATOL_F32, ATOL_F64, RTOL_F32, RTOL_F64, artifact_path, golden_index, golden_inputs
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+from grg_spmv_b200 import RuntimeRequirements  # noqa: E402
+
+
+def _req(k=8, **kw):
+    base = dict(max_k_up=k, max_k_down=k, need_down_miss_input=True, need_up_miss_output=True,
+                need_init_vector=True, need_init_matrix=True, need_init_xtx=True)
+    base.update(kw)
+    return RuntimeRequirements(**base)
+
+
+def _layout(paths, *, dtype=np.float64, req=None, exact=False, heavy=None, budget=0, ring=0, allow_residency=True, stream=0, pair=None):
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, plan_b200_layout
+
+    if pair is None:
+        kw = {} if heavy is None else {"heavy_threshold": heavy}
+        pair = B200PlanPair(plan_up=B200Plan(exact_order=exact, **kw), plan_down=B200Plan(exact_order=exact, **kw))
+    return plan_b200_layout(artifacts=list(paths), dtype=dtype, requirements=req or _req(), vram_budget_bytes=budget,
+                            ring_buffer_size=ring, allow_residency=allow_residency, device=0, stream=stream, pair=pair)
+
+
+def _run_case(grg, case, data):
+    x, init, miss = golden_inputs(case, data)
+    out = grg.matmul(x, case["direction"], emit_all_nodes=case["emit_all_nodes"], by_individual=case["by_individual"],
+                     init=init, miss=miss)
+    return out, miss
+
+
+def _cases_by_artifact():
+    groups: dict[tuple[str, str], list[dict]] = {}
+    for case in golden_index():
+        groups.setdefault((case["artifact"], case["dtype"]), []).append(case)
+    return groups
+
+
+GROUPS = _cases_by_artifact()
+
+
+@pytest.mark.parametrize("heavy", [128, 2], ids=["narrow", "heavy-rows"])
+@pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
+def test_golden_bit_exact_in_exact_order(group, heavy, golden_data):
+    """exact_order=True reproduces ReferenceRuntime bit for bit, for every golden case."""
+    from grg_spmv_b200.backends.b200 import B200Runtime
+
+    name, dtype = group
+    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=True, heavy=heavy)
+    with B200Runtime(layout, check_bounds=True) as runtime:
+        (grg,) = runtime.grgs
+        for case in GROUPS[group]:
+            out, miss = _run_case(grg, case, golden_data)
+            expected = golden_data[case["key"] + "|out"]
+            assert out.dtype == expected.dtype
+            np.testing.assert_array_equal(out, expected, err_msg=case["key"])
+            if case["miss"] and case["direction"] == "up":
+                np.testing.assert_array_equal(miss, golden_data[case["key"] + "|miss_out"], err_msg=case["key"])
+        assert runtime.device_error() == 0
+
+
+@pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
+def test_golden_fast_mode_heavy_rows(group, golden_data):
+    """Default (tree-reduced heavy rows): exact for integer-valued inputs, tolerance otherwise."""
+    from grg_spmv_b200.backends.b200 import B200Runtime
+
+    name, dtype = group
+    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=False, heavy=2)
+    rtol, atol = (RTOL_F64, ATOL_F64) if dtype == "float64" else (RTOL_F32, ATOL_F32)
+    with B200Runtime(layout, check_bounds=True) as runtime:
+        (grg,) = runtime.grgs
+        for case in GROUPS[group]:
+            out, _ = _run_case(grg, case, golden_data)
+            expected = golden_data[case["key"] + "|out"]
+            integer = any(tag in case["case"] for tag in ("pm1", "ones", "zeros"))
+            if integer and case["init"] is None:
+                np.testing.assert_array_equal(out, expected, err_msg=case["key"])
+            else:
+                np.testing.assert_allclose(out, expected, rtol=rtol, atol=atol * max(1.0, np.abs(expected).max()), err_msg=case["key"])
+        assert runtime.device_error() == 0
