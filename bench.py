@@ -56,7 +56,13 @@ def parse_args():
     p.add_argument("--exact-order", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--artifact", default=None, help="reuse an existing .grg_spmv instead of generating one")
+    p.add_argument("--no-clocks", action="store_true", help="skip clock sampling and its untimed busy loops")
+    p.add_argument("--artifact", default=None, help=".grg_spmv to use (generated there first if missing)")
+    p.add_argument("--heavy-threshold", type=int, default=None)
+    p.add_argument("--variant", type=int, default=None, help="narrow-row kernel variant")
+    p.add_argument("--no-graphs", action="store_true", help="launch kernels per level instead of replaying a CUDA graph")
+    p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
+    p.add_argument("--row-order-down", choices=["natural", "locality"], default=None)
     return p.parse_args()
 
 
@@ -72,9 +78,9 @@ def workload_spec(name: str, seed: int):
 def make_artifact(args, rank: int) -> tuple[Path, float]:
     from grg_spmv_b200.synth import write_synthetic_artifact
 
-    if args.artifact:
+    if args.artifact and Path(args.artifact).exists():
         return Path(args.artifact), 0.0
-    out = Path(tempfile.mkdtemp(prefix="grg_bench_")) / f"{args.workload}_r{rank}.grg_spmv"
+    out = Path(args.artifact) if args.artifact else Path(tempfile.mkdtemp(prefix="grg_bench_")) / f"{args.workload}_r{rank}.grg_spmv"
     t0 = time.perf_counter()
     write_synthetic_artifact(workload_spec(args.workload, seed=rank), out)
     return out, time.perf_counter() - t0
@@ -92,6 +98,8 @@ class ClockSampler:
         self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
 
     def __enter__(self):
+        if self.device_index < 0:
+            return self
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -170,18 +178,23 @@ def run_b200(args) -> None:
     from grg_spmv_b200 import RuntimeRequirements, scan_grg_spmv
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime, plan_b200_layout
     from grg_spmv_b200.backends.b200 import _native as nat
+    from grg_spmv_b200.types import Direction
 
     path, gen_s = make_artifact(args, rank)
     scan = scan_grg_spmv(path)
     k = int(args.k)
     req = RuntimeRequirements(max_k_up=k, max_k_down=k, need_down_miss_input=True, need_up_miss_output=False,
                               need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
-    pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order), plan_down=B200Plan(exact_order=args.exact_order))
+    extra = {} if args.heavy_threshold is None else {"heavy_threshold": args.heavy_threshold}
+    if args.variant is not None:
+        extra["narrow_variant"] = args.variant
+    pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
+                        plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
     stream = torch.cuda.Stream(device=device)
     layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
                               device=local_rank, stream=stream, pair=pair)
     t0 = time.perf_counter()
-    runtime = B200Runtime(layout).__enter__()
+    runtime = B200Runtime(layout, use_graphs=not args.no_graphs).__enter__()
     enter_s = time.perf_counter() - t0
     (grg,) = runtime.grgs
     S, M, E = grg.num_samples, grg.num_mutations, grg.num_edges
@@ -218,16 +231,18 @@ def run_b200(args) -> None:
                     step()
                 torch.cuda.synchronize(device)
 
-        with ClockSampler(local_rank) as clocks:
-            clocks.wait_for_samples(1)
-            busy(0.6)
+        with ClockSampler(local_rank if not args.no_clocks else -1) as clocks:
+            if not args.no_clocks:
+                clocks.wait_for_samples(1)
+                busy(0.6)
             synced_barrier()
             start.record(stream)
             for _ in range(args.steps):
                 step()
             end.record(stream)
             synced_barrier()
-            busy(0.6)
+            if not args.no_clocks:
+                busy(0.6)
         elapsed_ms = start.elapsed_time(end)
     max_ms = elapsed_ms
     total_work = args.steps * 2.0 * E * k
@@ -353,6 +368,10 @@ def run_b200(args) -> None:
                                    f"1% missing, fully resident, up+down per step",
                        "k": k, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
+                       "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": pair.plan_down.narrow_variant,
+                       "cuda_graphs": not args.no_graphs,
+                       "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
+                                     "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
                        "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": "level gather (level_narrow_kernel + level_wide_kernel)",

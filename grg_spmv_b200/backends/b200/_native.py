@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 1
+ABI_VERSION = 3
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -36,6 +36,7 @@ SRC_SHIFT = 29
 SRC_STATE, SRC_INPUT, SRC_MISS = 0, 1, 2
 ID_MASK = 0x1FFFFFFF
 MAX_ID = 0x1FFFFFFF
+NARROW_VARIANTS = 5
 
 
 class Level(ctypes.Structure):
@@ -45,11 +46,12 @@ class Level(ctypes.Structure):
         ("num_entries", ctypes.c_int64),
         ("num_heavy", ctypes.c_int64),
         ("heavy_threshold", ctypes.c_int32),
-        ("slot", ctypes.c_int32),
+        ("ring_slot", ctypes.c_int32),
         ("blob", ctypes.c_void_p),
         ("blob_bytes", ctypes.c_int64),
         ("off_row_ptr", ctypes.c_int64),
         ("off_heavy", ctypes.c_int64),
+        ("off_row_ids", ctypes.c_int64),
         ("off_entries", ctypes.c_int64),
     ]
 
@@ -99,6 +101,7 @@ class TraverseArgs(ctypes.Structure):
         ("slot_bytes", ctypes.POINTER(ctypes.c_int64)),
         ("num_slots", ctypes.c_int32),
         ("error_word", ctypes.c_void_p),
+        ("narrow_variant", ctypes.c_int32),
     ]
 
 

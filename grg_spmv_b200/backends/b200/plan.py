@@ -57,23 +57,38 @@ class B200Plan:
     bit-identical to the reference's ReferenceRuntime (default: heavy rows are split over a
     CTA and tree-reduced, deterministic and exact for integer-valued data).
     ``heavy_threshold``: rows with more entries than this are processed one CTA per row.
+    ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
+    processed together); None picks the direction's default (up natural, down locality).
+    ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``).
     """
 
     exact_order: bool = False
     heavy_threshold: int = DEFAULT_HEAVY_THRESHOLD
+    row_order: str | None = None
+    narrow_variant: int = 0
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
+        if self.row_order not in (None, "natural", "locality"):
+            raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
+        if not 0 <= int(self.narrow_variant) < 5:
+            raise ValueError(f"narrow_variant must be in [0, 5), got {self.narrow_variant}")
+
+    def locality(self, direction: Direction) -> bool:
+        if self.row_order is None:
+            return direction == Direction.DOWN
+        return self.row_order == "locality"
 
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
-        allowed = {"exact_order", "heavy_threshold"}
+        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
         return cls(exact_order=bool(value.get("exact_order", False)),
-                   heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)))
+                   heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)),
+                   row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 0)))
 
 
 @dataclass(frozen=True)
@@ -250,7 +265,7 @@ def _level_plans(artifact_index: int, scan: ArtifactScan, direction: Direction, 
             continue
         entries = up_entry_bound(scan, level) if direction == Direction.UP else down_entry_bound(scan, level, with_miss)
         heavy = min(rows, entries // (int(plan.heavy_threshold) + 1))
-        nbytes = blob_layout(rows, heavy, entries)[3]
+        nbytes = blob_layout(rows, heavy, entries, True)[4]  # row map: locality order or heavy suffix
         out.append(LevelPlan(artifact_index, direction, level, pos, rows, entries, heavy, nbytes))
     return tuple(out)
 

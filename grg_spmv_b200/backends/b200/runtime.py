@@ -13,6 +13,9 @@ Mirrors ``TritonRuntime`` (``pygrgl_spmv/backends/triton/backend.py:609-1225``) 
 * A call runs asynchronously on the layout's caller stream, ordered after earlier work on
   that stream; it allocates nothing and never synchronises the host, so it can be captured
   in a CUDA graph.  Concurrent calls on one runtime fail fast (``:773-783``).
+* Each prepared op records its traversal as a CUDA graph when it is prepared (unless the
+  caller's stream is capturing) and replays it on every call: one graph launch instead of one
+  kernel launch per level.
 
 The whole prepared call is one C-ABI call, ``grg_b200_traverse`` (``include/grg_b200.h``):
 seed, one fused gather pass per level, output stage.  There is no CPU or PyTorch fallback.
@@ -107,6 +110,7 @@ class B200PreparedMatmul:
             self.init_matrix = init_matrix.T
         self._args = runtime._traverse_args(artifact, spec, self._input_internal, self._output_internal, miss_view,
                                             init_vector, init_matrix)
+        self._graph = runtime._capture(self._args)
 
     def __enter__(self) -> "B200PreparedMatmul":
         return self
@@ -119,7 +123,7 @@ class B200PreparedMatmul:
             self._call_prelocked()
 
     def _call_prelocked(self) -> None:
-        self._runtime._launch(self._args)
+        self._runtime._launch(self._args, self._graph)
 
 
 class B200Runtime:
@@ -127,7 +131,7 @@ class B200Runtime:
 
     _bound_grg_cls = BoundGRG
 
-    def __init__(self, layout: B200Layout, *, check_bounds: bool | None = None) -> None:
+    def __init__(self, layout: B200Layout, *, check_bounds: bool | None = None, use_graphs: bool | None = None) -> None:
         import torch
 
         if not torch.cuda.is_available():
@@ -141,6 +145,9 @@ class B200Runtime:
         if check_bounds is None:
             check_bounds = os.environ.get("GRG_B200_CHECK_BOUNDS", "0") not in ("", "0")
         self._check_bounds = bool(check_bounds)
+        if use_graphs is None:
+            use_graphs = os.environ.get("GRG_B200_GRAPHS", "1") not in ("", "0")
+        self._use_graphs = bool(use_graphs)
         self._reset_owned_state()
 
     # -- lifecycle ----------------------------------------------------------------------------
@@ -266,12 +273,15 @@ class B200Runtime:
         levels = {}
         off = np.asarray(st.level_offsets, dtype=np.int64)
         if up_on:
-            built = {lv.level: lv for lv in build_up_levels(off, coo, lay.pair.plan_up.heavy_threshold)}
+            plan = lay.pair.plan_up
+            built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP))}
             levels[Direction.UP] = self._upload_levels(art.levels_up, built)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
+            plan = lay.pair.plan_down
             built = {lv.level: lv for lv in build_down_levels(
-                off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, lay.pair.plan_down.heavy_threshold)}
+                off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
+                plan.locality(Direction.DOWN))}
             levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
         del coo
         return _DeviceArtifact(
@@ -299,7 +309,7 @@ class B200Runtime:
         keep = []
         for i, lp in enumerate(plans):
             lv = built[lp.level]
-            off_ptr, off_heavy, off_entries, nbytes = lv.layout()
+            off_ptr, off_heavy, off_ids, off_entries, nbytes = lv.layout()
             if nbytes > lp.nbytes:
                 raise RuntimeError(f"level {lp.level} needs {nbytes} bytes, more than the {lp.nbytes} planned")
             blob = torch.from_numpy(lv.pack())
@@ -311,9 +321,9 @@ class B200Runtime:
                 slot = int(lp.slot)
             keep.append(blob)
             arr[i] = nat.Level(row_begin=lv.row_begin, num_rows=lv.num_rows, num_entries=lv.num_entries,
-                               num_heavy=int(lv.heavy_rows.size), heavy_threshold=lv.heavy_threshold, slot=slot,
+                               num_heavy=int(lv.heavy_rows.size), heavy_threshold=lv.heavy_threshold, ring_slot=slot,
                                blob=blob.data_ptr(), blob_bytes=nbytes, off_row_ptr=off_ptr, off_heavy=off_heavy,
-                               off_entries=off_entries)
+                               off_row_ids=off_ids, off_entries=off_entries)
         return _DeviceLevels(array=arr, keepalive=keep)
 
     # -- calls ----------------------------------------------------------------------------------
@@ -403,12 +413,43 @@ class B200Runtime:
             a.slot_bytes = ctypes.cast(self._slot_bytes, ctypes.POINTER(ctypes.c_int64))
             a.num_slots = len(self._slots)
         a.error_word = _ptr(self._error_word) if self._check_bounds else None
+        a.narrow_variant = int(plan.narrow_variant)
         return a
 
-    def _launch(self, args: nat.TraverseArgs) -> None:
+    def _capturing(self) -> bool:
+        import torch
+
+        with torch.cuda.device(self.device), torch.cuda.stream(self._caller_stream):
+            return bool(torch.cuda.is_current_stream_capturing())
+
+    def _capture(self, args: nat.TraverseArgs):
+        """Record one traversal as a CUDA graph (replayed by every later call: one launch
+        instead of one per level).  Skipped when graphs are off or the caller's stream is
+        itself being captured, in which case calls launch the kernels into that capture."""
+        import torch
+
+        if not self._use_graphs or self._capturing():
+            return None
+        with torch.cuda.device(self.device):
+            graph = torch.cuda.CUDAGraph()
+            side = torch.cuda.Stream(device=self.device)
+            with torch.cuda.stream(side):
+                graph.capture_begin(capture_error_mode="thread_local")
+                try:
+                    status = self._lib.grg_b200_traverse(ctypes.byref(args), ctypes.c_void_p(side.cuda_stream))
+                finally:
+                    graph.capture_end()
+        nat.check(self._lib, status, "grg_b200_traverse (graph capture)")
+        return graph
+
+    def _launch(self, args: nat.TraverseArgs, graph=None) -> None:
         import torch
 
         with torch.cuda.device(self.device):
+            if graph is not None and not self._capturing():
+                with torch.cuda.stream(self._caller_stream):
+                    graph.replay()
+                return
             status = self._lib.grg_b200_traverse(ctypes.byref(args), ctypes.c_void_p(self.stream_ptr))
         nat.check(self._lib, status, "grg_b200_traverse")
 

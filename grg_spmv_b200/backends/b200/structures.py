@@ -16,8 +16,12 @@ left-to-right sum with a fresh partial sum per segment reproduces ``ReferenceRun
 
 Blocks are canonicalised first (duplicates merged, columns sorted), as the reference does in
 ``materialize_sparse_block`` (``pygrgl_spmv/backends/base.py:128-139``).  Each level is packed
-into one byte blob ``[int32 row_ptr | int32 heavy_rows | uint32 entries]`` with 16-byte
+into one byte blob ``[int32 row_ptr | int32 heavy_rows | int32 row_ids | uint32 entries]`` with 16-byte
 aligned sections, the unit of residency and of streaming through the ring.
+
+Rows may be stored in a locality order instead of node order (``row_ids`` maps processing
+position to row): the kernels' results do not depend on the order in which rows are
+processed, only on each row's own list.
 """
 
 from __future__ import annotations
@@ -35,37 +39,49 @@ def _align(n: int) -> int:
     return (int(n) + ALIGN - 1) // ALIGN * ALIGN
 
 
-def blob_layout(num_rows: int, num_heavy: int, num_entries: int) -> tuple[int, int, int, int]:
-    """(off_row_ptr, off_heavy, off_entries, blob_bytes) of a level blob."""
+def blob_layout(num_rows: int, num_heavy: int, num_entries: int, with_row_ids: bool) -> tuple[int, int, int, int, int]:
+    """(off_row_ptr, off_heavy, off_row_ids or -1, off_entries, blob_bytes) of a level blob."""
     off_heavy = _align(4 * (int(num_rows) + 1))
-    off_entries = off_heavy + _align(4 * int(num_heavy))
-    return 0, off_heavy, off_entries, off_entries + _align(4 * max(int(num_entries), 1))
+    off_ids = off_heavy + _align(4 * int(num_heavy))
+    off_entries = off_ids + (_align(4 * int(num_rows)) if with_row_ids else 0)
+    return 0, off_heavy, (off_ids if with_row_ids else -1), off_entries, off_entries + _align(4 * max(int(num_entries), 1))
 
 
 @dataclass
 class LevelGather:
+    """One level's gather lists in processing order (position p computes row ``row_ids[p]``)."""
+
     level: int
     row_begin: int
     num_rows: int
-    row_ptr: np.ndarray  # int32 [num_rows + 1]
+    row_ptr: np.ndarray  # int32 [num_rows + 1], by processing position
     entries: np.ndarray  # uint32
-    heavy_rows: np.ndarray  # int32
+    heavy_rows: np.ndarray  # int32 processing positions
     heavy_threshold: int
+    row_ids: np.ndarray | None = None  # int32 level-local row of each position (None: identity)
 
     @property
     def num_entries(self) -> int:
         return int(self.entries.size)
 
-    def layout(self) -> tuple[int, int, int, int]:
-        return blob_layout(self.num_rows, self.heavy_rows.size, self.entries.size)
+    def layout(self) -> tuple[int, int, int, int, int]:
+        return blob_layout(self.num_rows, self.heavy_rows.size, self.entries.size, self.row_ids is not None)
 
     def pack(self) -> np.ndarray:
-        off_ptr, off_heavy, off_entries, nbytes = self.layout()
+        off_ptr, off_heavy, off_ids, off_entries, nbytes = self.layout()
         blob = np.zeros(nbytes, dtype=np.uint8)
         blob[off_ptr:off_ptr + 4 * self.row_ptr.size] = self.row_ptr.view(np.uint8)
         blob[off_heavy:off_heavy + 4 * self.heavy_rows.size] = self.heavy_rows.view(np.uint8)
+        if self.row_ids is not None:
+            blob[off_ids:off_ids + 4 * self.row_ids.size] = self.row_ids.view(np.uint8)
         blob[off_entries:off_entries + 4 * self.entries.size] = self.entries.view(np.uint8)
         return blob
+
+    def row_lists(self):
+        """(level-local row, entries) per processing position (test helper)."""
+        for p in range(self.num_rows):
+            row = p if self.row_ids is None else int(self.row_ids[p])
+            yield row, self.entries[int(self.row_ptr[p]):int(self.row_ptr[p + 1])]
 
 
 def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.ndarray, np.ndarray]:
@@ -82,8 +98,13 @@ def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.nd
 
 
 def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
-            group: np.ndarray, heavy_threshold: int) -> LevelGather:
-    """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr."""
+            group: np.ndarray, heavy_threshold: int, locality: bool = False) -> LevelGather:
+    """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr.
+
+    With ``locality`` the rows are stored in the order of the id of their last state entry
+    (the lowest-level parent for down), so rows that share source rows are processed close
+    together and the shared rows are fetched from L2; each row still writes its own slot.
+    """
     order = np.argsort(rows, kind="stable")
     rows, ids, src, group = rows[order], ids[order], src[order], group[order]
     if ids.size and int(ids.max()) > nat.MAX_ID:
@@ -97,10 +118,30 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
     if ids.size > 1:
         start[1:] = (rows[1:] != rows[:-1]) | (group[1:] != group[:-1])
     entries = (ids.astype(np.uint32) | (src.astype(np.uint32) << np.uint32(nat.SRC_SHIFT))
-               | np.where(start, np.uint32(nat.SEG_START), np.uint32(0)))
-    heavy = np.flatnonzero(counts > heavy_threshold).astype(np.int32)
-    return LevelGather(level, int(row_begin), int(num_rows), row_ptr.astype(np.int32), entries.astype(np.uint32),
-                       heavy, int(heavy_threshold))
+               | np.where(start, np.uint32(nat.SEG_START), np.uint32(0))).astype(np.uint32)
+    # Processing order: narrow rows first (in locality order when asked), heavy rows last.
+    perm = np.arange(num_rows, dtype=np.int64)
+    if locality and num_rows > 1:
+        key = np.full(num_rows, np.iinfo(np.int64).max, dtype=np.int64)
+        state_pos = np.flatnonzero(src == nat.SRC_STATE)
+        # Last state entry of each row: first occurrence in the reversed (row-sorted) list.
+        uniq, first_rev = np.unique(rows[state_pos][::-1], return_index=True)
+        key[uniq] = ids[state_pos[::-1][first_rev]]
+        perm = np.argsort(key, kind="stable")
+    heavy_mask = counts[perm] > heavy_threshold
+    perm = np.concatenate((perm[~heavy_mask], perm[heavy_mask]))
+    num_heavy = int(heavy_mask.sum())
+    row_ids = None
+    if not np.array_equal(perm, np.arange(num_rows)):
+        lengths = counts[perm]
+        new_ptr = np.zeros(num_rows + 1, dtype=np.int64)
+        np.cumsum(lengths, out=new_ptr[1:])
+        gather = np.repeat(row_ptr[:-1][perm] - new_ptr[:-1], lengths) + np.arange(int(new_ptr[-1]), dtype=np.int64)
+        entries = entries[gather]
+        row_ptr, row_ids = new_ptr, perm.astype(np.int32)
+    heavy = np.arange(num_rows - num_heavy, num_rows, dtype=np.int32)
+    return LevelGather(level, int(row_begin), int(num_rows), row_ptr.astype(np.int32), entries, heavy,
+                       int(heavy_threshold), row_ids)
 
 
 def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
@@ -113,7 +154,7 @@ def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
     return out
 
 
-def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int) -> list[LevelGather]:
+def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, locality: bool = False) -> list[LevelGather]:
     """Gather lists for up levels 1..h-1 (level 0 is seeded from the input)."""
     off = np.asarray(level_offsets, dtype=np.int64)
     h = off.size - 1
@@ -130,7 +171,7 @@ def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int) 
             src.append(np.full(r.size, s, dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
-        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold))
+        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality))
     return levels
 
 
@@ -143,7 +184,8 @@ def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[
     return nodes[order], muts[order]
 
 
-def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int) -> list[LevelGather]:
+def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int,
+                      locality: bool = True) -> list[LevelGather]:
     """Gather lists for down levels h-1..0 in execution order.
 
     ``sel_mut``/``sel_miss`` are (indptr, indices, num_mutations) triples; ``sel_miss`` may be
@@ -176,7 +218,7 @@ def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, h
             grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         levels.append(_finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
-                              cat(grp, np.int16), heavy_threshold))
+                              cat(grp, np.int16), heavy_threshold, locality))
     return levels
 
 

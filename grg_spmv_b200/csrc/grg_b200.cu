@@ -133,6 +133,7 @@ struct LevelArgs {
     const int32_t* row_ptr;
     const uint32_t* entries;
     const int32_t* heavy_rows;
+    const int32_t* row_ids;
     int64_t num_heavy;
     int32_t heavy_threshold;
     int32_t use_miss;
@@ -215,23 +216,56 @@ __device__ __forceinline__ const T* entry_row(const LevelArgs& a, uint32_t code)
 // ---------------------------------------------------------------------------------------
 // Level kernels
 // ---------------------------------------------------------------------------------------
-template <typename T, int V, int INIT>
-__global__ void __launch_bounds__(256) level_narrow_kernel(LevelArgs a) {
-    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    const int64_t local = t >> a.log2g;
-    if (local >= a.num_rows) return;
-    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
-    const int32_t e0 = __ldg(a.row_ptr + local);
-    const int32_t e1 = __ldg(a.row_ptr + local + 1);
-    if (e1 - e0 > a.heavy_threshold) return;  // handled by level_wide_kernel
-    const int64_t row = a.row_begin + local;
+constexpr int kNarrowThreads = 256;
+constexpr int kNarrowWarps = kNarrowThreads / 32;
+constexpr int kStageCap = 1024;  // gather-list entries staged in shared memory per warp
+constexpr unsigned kFullMask = 0xffffffffu;
+
+__device__ __forceinline__ int64_t level_row(const LevelArgs& a, int64_t pos) {
+    return a.row_begin + (a.row_ids ? static_cast<int64_t>(__ldg(a.row_ids + pos)) : pos);
+}
+
+// Narrow rows.  A warp owns 32/G consecutive processing positions; lane group g (G lanes)
+// owns position g and columns [lane*V, lane*V + V) (+ multiples of G*V).  The warp first
+// copies the gather-list span of its positions into shared memory with coalesced loads;
+// each lane then fetches U rows at a time (independent loads) and adds them in list order,
+// restarting the partial sum at every segment start.
+//
+// Variants (``narrow_variant``): U = rows fetched per round, STAGE = shared-memory staging.
+template <typename T, int V, int INIT, int U, bool STAGE>
+__global__ void __launch_bounds__(kNarrowThreads) level_narrow_kernel(LevelArgs a) {
+    __shared__ uint32_t stage[kNarrowWarps][STAGE ? kStageCap : 1];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int rpw_log = 5 - a.log2g;  // positions per warp = 32 >> log2g
+    const int64_t pos0 = (static_cast<int64_t>(blockIdx.x) * kNarrowWarps + warp) << rpw_log;
+    if (pos0 >= a.num_rows) return;  // uniform across the warp
+    const int here = static_cast<int>(a.num_rows - pos0 < (int64_t(1) << rpw_log) ? a.num_rows - pos0 : (int64_t(1) << rpw_log));
+    // Lane l < here holds the list bounds of position pos0 + l (a full warp of single-lane
+    // rows needs 33 offsets, so each lane loads both ends of its own position).
+    int32_t lo = 0, hi = 0;
+    if (lane < here) {
+        lo = __ldg(a.row_ptr + pos0 + lane);
+        hi = __ldg(a.row_ptr + pos0 + lane + 1);
+    }
+    const int32_t span_begin = __shfl_sync(kFullMask, lo, 0);
+    const int32_t span = __shfl_sync(kFullMask, hi, here - 1) - span_begin;
+    const int my = lane >> a.log2g;
+    const int owner = my < here ? my : 0;
+    const int32_t e0 = __shfl_sync(kFullMask, lo, owner);
+    const int32_t e1 = __shfl_sync(kFullMask, hi, owner);
+    const bool staged = STAGE && span <= kStageCap;
+    if (staged) {
+        for (int j = lane; j < span; j += 32) stage[warp][j] = __ldg(a.entries + span_begin + j);
+    }
+    __syncwarp();
+    if (my >= here || e1 - e0 > a.heavy_threshold) return;  // heavy rows: level_wide_kernel
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int64_t row = level_row(a, pos0 + my);
     T* state = static_cast<T*>(a.state);
+    const uint32_t* stage_w = stage[warp];
     const int64_t step = static_cast<int64_t>(V) << a.log2g;
-    // Entries are consumed U at a time: all U codes are loaded, then all U rows, then the U
-    // values are added in list order.  The adds keep the reference's order; the loads of a
-    // chunk are independent, so U row fetches are in flight per lane instead of one.
-    constexpr int U = (V == 1) ? 8 : 4;
-    for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step) {
+    for (int64_t c = static_cast<int64_t>(glane) * V; c < a.k; c += step) {
         Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
         Pack<T, V> seg = zero_pack<T, V>();
         for (int32_t e = e0; e < e1; e += U) {
@@ -239,7 +273,10 @@ __global__ void __launch_bounds__(256) level_narrow_kernel(LevelArgs a) {
             Pack<T, V> val[U];
             bool valid[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) code[u] = (e + u < e1) ? __ldg(a.entries + e + u) : 0u;
+            for (int u = 0; u < U; ++u) {
+                const int32_t eu = e + u;
+                code[u] = eu >= e1 ? 0u : (staged ? stage_w[eu - span_begin] : __ldg(a.entries + eu));
+            }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const T* src = (e + u < e1) ? entry_row<T>(a, code[u]) : nullptr;
@@ -260,18 +297,120 @@ __global__ void __launch_bounds__(256) level_narrow_kernel(LevelArgs a) {
     }
 }
 
-constexpr int kWideThreads = 128;
+// cp.async helpers: global -> shared copies that hold no registers while in flight.
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    if constexpr (BYTES == 16) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(dst), "l"(gmem), "n"(BYTES) : "memory");
+    }
+}
 
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+constexpr int kAsyncWarps = 4;
+constexpr int kAsyncThreads = kAsyncWarps * 32;
+constexpr int kAsyncValBytes = 8192;  // gathered row segments per warp and round
+constexpr int kAsyncCodeCap = 512;    // list entries per warp and round
+
+// Narrow rows, asynchronous gathers (narrow_variant 4).  Same ownership as
+// level_narrow_kernel (a warp owns 32/G positions, lane group g owns position g).  Per round
+// the warp copies up to `cap` list entries of its span into shared memory, issues one
+// cp.async per (entry, lane) for the entry's row segment [c0 + lane*V, +V), waits once, and
+// every lane group then adds its own row's entries from shared memory in list order.  All row
+// fetches of a round are in flight at once without occupying registers.
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kAsyncThreads) level_async_kernel(LevelArgs a) {
+    __shared__ __align__(16) unsigned char vals_raw[kAsyncWarps][kAsyncValBytes];
+    __shared__ uint32_t codes_s[kAsyncWarps][kAsyncCodeCap];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int rpw_log = 5 - a.log2g;
+    const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
+    const int64_t pos0 = (static_cast<int64_t>(blockIdx.x) * kAsyncWarps + warp) << rpw_log;
+    if (pos0 >= narrow) return;  // uniform across the warp
+    const int here = static_cast<int>(narrow - pos0 < (int64_t(1) << rpw_log) ? narrow - pos0 : (int64_t(1) << rpw_log));
+    int32_t lo = 0, hi = 0;
+    if (lane < here) {
+        lo = __ldg(a.row_ptr + pos0 + lane);
+        hi = __ldg(a.row_ptr + pos0 + lane + 1);
+    }
+    const int32_t span_begin = __shfl_sync(kFullMask, lo, 0);
+    const int32_t span_end = __shfl_sync(kFullMask, hi, here - 1);
+    const int my = lane >> a.log2g;
+    const int owner = my < here ? my : 0;
+    const int32_t e0 = __shfl_sync(kFullMask, lo, owner);
+    const int32_t e1 = __shfl_sync(kFullMask, hi, owner);
+    const bool has_row = my < here;
+    const int g_lanes = 1 << a.log2g;
+    const int g = lane & (g_lanes - 1);
+    const int64_t row = has_row ? level_row(a, pos0 + my) : 0;
+    Pack<T, V>* vals = reinterpret_cast<Pack<T, V>*>(vals_raw[warp]);
+    uint32_t* codes = codes_s[warp];
+    const int per_entry = static_cast<int>(sizeof(T)) * V << a.log2g;
+    const int cap = kAsyncValBytes / per_entry < kAsyncCodeCap ? kAsyncValBytes / per_entry : kAsyncCodeCap;
+    T* state = static_cast<T*>(a.state);
+    const int64_t cstep = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c0 = 0; c0 < a.k; c0 += cstep) {
+        const int64_t c = c0 + static_cast<int64_t>(g) * V;
+        const bool live = has_row && c < a.k;
+        Pack<T, V> acc = live ? init_value<T, V, INIT>(a, row, c) : zero_pack<T, V>();
+        Pack<T, V> seg = zero_pack<T, V>();
+        for (int32_t sub = span_begin; sub < span_end; sub += cap) {
+            const int n = span_end - sub < cap ? span_end - sub : cap;
+            for (int j = lane; j < n; j += 32) codes[j] = __ldg(a.entries + sub + j);
+            __syncwarp();
+            for (int q = lane; q < (n << a.log2g); q += 32) {
+                const int j = q >> a.log2g;
+                const int64_t cc = c0 + static_cast<int64_t>(q & (g_lanes - 1)) * V;
+                const T* src = entry_row<T>(a, codes[j]);
+                if (src && cc < a.k) cp_async<static_cast<int>(sizeof(T)) * V>(&vals[q], src + cc);
+            }
+            cp_async_wait_all();
+            __syncwarp();
+            if (live) {
+                const int32_t lo_e = e0 > sub ? e0 : sub;
+                const int32_t hi_e = e1 < sub + n ? e1 : sub + n;
+                for (int32_t e = lo_e; e < hi_e; ++e) {
+                    const uint32_t code = codes[e - sub];
+                    if (code & GRG_B200_SEG_START) {
+                        add_into(acc, seg);
+                        seg = zero_pack<T, V>();
+                    }
+                    if (entry_row<T>(a, code)) add_into(seg, vals[((e - sub) << a.log2g) + g]);
+                }
+            }
+            __syncwarp();
+        }
+        if (live) {
+            add_into(acc, seg);
+            st_pack(state + row * a.ld_state + c, acc);
+        }
+    }
+}
+
+constexpr int kWideThreads = 128;
+constexpr int kWideChunk = 512;  // gather-list entries staged per round
+
+// Heavy rows, one CTA each.  Default: the CTA stages the list in chunks, entry groups of G
+// lanes fetch rows independently, and the partial sums are tree-reduced in a fixed order
+// (deterministic; exact whenever the data are integers).  EXACT: chunks are fetched in
+// parallel but added by one lane group in list order (bit-identical to the reference).
 template <typename T, int V, int INIT, bool EXACT>
 __global__ void __launch_bounds__(kWideThreads) level_wide_kernel(LevelArgs a) {
     __shared__ Pack<T, V> red[kWideThreads];
-    __shared__ uint32_t codes[kWideThreads];
-    const int64_t local = __ldg(a.heavy_rows + blockIdx.x);
-    const int32_t e0 = __ldg(a.row_ptr + local);
-    const int32_t e1 = __ldg(a.row_ptr + local + 1);
-    const int64_t row = a.row_begin + local;
-    const int g_lanes = 1 << a.log2g;                // lanes per column group
-    const int groups = kWideThreads >> a.log2g;      // entry groups
+    __shared__ uint32_t codes[kWideChunk];
+    const int64_t pos = __ldg(a.heavy_rows + blockIdx.x);
+    const int32_t e0 = __ldg(a.row_ptr + pos);
+    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
+    const int64_t row = level_row(a, pos);
+    const int g_lanes = 1 << a.log2g;
+    const int groups = kWideThreads >> a.log2g;
     const int lane = threadIdx.x & (g_lanes - 1);
     const int grp = threadIdx.x >> a.log2g;
     T* state = static_cast<T*>(a.state);
@@ -280,11 +419,25 @@ __global__ void __launch_bounds__(kWideThreads) level_wide_kernel(LevelArgs a) {
         const int64_t c = base + static_cast<int64_t>(lane) * V;
         const bool active = c < a.k;
         if constexpr (!EXACT) {
+            constexpr int UW = 4;
             Pack<T, V> part = zero_pack<T, V>();
-            if (active) {
-                for (int32_t e = e0 + grp; e < e1; e += groups) {
-                    const T* src = entry_row<T>(a, __ldg(a.entries + e));
-                    if (src) add_into(part, ld_ro<T, V>(src + c));
+            for (int32_t s0 = e0; s0 < e1; s0 += kWideChunk) {
+                const int n = min(kWideChunk, e1 - s0);
+                __syncthreads();
+                for (int j = threadIdx.x; j < n; j += kWideThreads) codes[j] = __ldg(a.entries + s0 + j);
+                __syncthreads();
+                if (active) {
+                    for (int j = grp; j < n; j += groups * UW) {
+                        Pack<T, V> val[UW];
+#pragma unroll
+                        for (int u = 0; u < UW; ++u) {
+                            const int jj = j + u * groups;
+                            const T* src = jj < n ? entry_row<T>(a, codes[jj]) : nullptr;
+                            val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                        }
+#pragma unroll
+                        for (int u = 0; u < UW; ++u) add_into(part, val[u]);
+                    }
                 }
             }
             red[threadIdx.x] = part;
@@ -503,6 +656,8 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->num_nodes > (int64_t)GRG_B200_MAX_ID + 1 || a->num_mutations > (int64_t)GRG_B200_MAX_ID + 1)
         return fail(GRG_B200_ERR_UNSUPPORTED, "node/mutation counts above %u are not supported", GRG_B200_MAX_ID + 1u);
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
+    if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
+        return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
     if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
     if (a->init_mode == GRG_B200_INIT_XTX && !a->xtx_node) return fail(GRG_B200_ERR_INVALID, "xtx_node is NULL");
     if (a->init_mode == GRG_B200_INIT_MATRIX && (!a->init_matrix || !a->node_perm || a->ld_init < a->k))
@@ -537,15 +692,37 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
 }
 
 template <typename T, int V>
-int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, cudaStream_t s) {
-    if (la.num_rows > 0) {
-        const dim3 grid = grid_for(la.num_rows, la.log2g, 256);
+int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, cudaStream_t s) {
+    const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
+    if (narrow > 0 && variant == 4) {
+        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        const dim3 grid(static_cast<unsigned>((warps + kAsyncWarps - 1) / kAsyncWarps));
         switch (init_mode) {
-            case 0: level_narrow_kernel<T, V, 0><<<grid, 256, 0, s>>>(la); break;
-            case 1: level_narrow_kernel<T, V, 1><<<grid, 256, 0, s>>>(la); break;
-            case 2: level_narrow_kernel<T, V, 2><<<grid, 256, 0, s>>>(la); break;
-            default: level_narrow_kernel<T, V, 3><<<grid, 256, 0, s>>>(la); break;
+            case 0: level_async_kernel<T, V, 0><<<grid, kAsyncThreads, 0, s>>>(la); break;
+            case 1: level_async_kernel<T, V, 1><<<grid, kAsyncThreads, 0, s>>>(la); break;
+            case 2: level_async_kernel<T, V, 2><<<grid, kAsyncThreads, 0, s>>>(la); break;
+            default: level_async_kernel<T, V, 3><<<grid, kAsyncThreads, 0, s>>>(la); break;
         }
+        GRG_LAUNCH_CHECK("level_async_kernel");
+    } else if (narrow > 0) {
+        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
+#define GRG_NARROW(INIT, U, ST) level_narrow_kernel<T, V, INIT, U, ST><<<grid, kNarrowThreads, 0, s>>>(la)
+#define GRG_NARROW_INIT(U, ST)                  \
+    switch (init_mode) {                        \
+        case 0: GRG_NARROW(0, U, ST); break;    \
+        case 1: GRG_NARROW(1, U, ST); break;    \
+        case 2: GRG_NARROW(2, U, ST); break;    \
+        default: GRG_NARROW(3, U, ST); break;   \
+    }
+        switch (variant) {
+            case 1: GRG_NARROW_INIT(8, false) break;
+            case 2: GRG_NARROW_INIT(4, true) break;
+            case 3: GRG_NARROW_INIT(16, true) break;
+            default: GRG_NARROW_INIT(4, false) break;
+        }
+#undef GRG_NARROW_INIT
+#undef GRG_NARROW
         GRG_LAUNCH_CHECK("level_narrow_kernel");
     }
     if (la.num_heavy > 0) {
@@ -591,11 +768,12 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     la.row_ptr = reinterpret_cast<const int32_t*>(base + L->off_row_ptr);
     la.entries = reinterpret_cast<const uint32_t*>(base + L->off_entries);
     la.heavy_rows = reinterpret_cast<const int32_t*>(base + L->off_heavy);
+    la.row_ids = L->off_row_ids >= 0 ? reinterpret_cast<const int32_t*>(base + L->off_row_ids) : nullptr;
     la.num_heavy = L->num_heavy;
     la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
     const bool exact = a->exact_order != 0;
     return dispatch(a, sh, [&](auto t, auto v) {
-        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, s);
+        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, s);
     });
 }
 
@@ -821,13 +999,13 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
     bool any_streamed = false;
     for (int i = 0; i < a->num_levels; ++i) {
         const grg_b200_level& L = a->levels[i];
-        if (L.slot >= 0) {
+        if (L.ring_slot >= 0) {
             any_streamed = true;
-            if (!a->ring || L.slot >= a->num_slots || L.slot >= a->ring->num_slots || !a->slot_buffers || !a->slot_bytes)
-                return fail(GRG_B200_ERR_INVALID, "level %d is streamed through slot %d but the ring is missing or too small", i, L.slot);
-            if (L.blob_bytes > a->slot_bytes[L.slot])
+            if (!a->ring || L.ring_slot >= a->num_slots || L.ring_slot >= a->ring->num_slots || !a->slot_buffers || !a->slot_bytes)
+                return fail(GRG_B200_ERR_INVALID, "level %d is streamed through slot %d but the ring is missing or too small", i, L.ring_slot);
+            if (L.blob_bytes > a->slot_bytes[L.ring_slot])
                 return fail(GRG_B200_ERR_INVALID, "level %d needs %lld bytes, slot %d has %lld", i, (long long)L.blob_bytes,
-                            L.slot, (long long)a->slot_bytes[L.slot]);
+                            L.ring_slot, (long long)a->slot_bytes[L.ring_slot]);
         }
     }
 
@@ -846,19 +1024,19 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
     for (int i = 0; i < a->num_levels; ++i) {
         const grg_b200_level& L = a->levels[i];
         const void* blob = L.blob;
-        if (L.slot >= 0 && L.num_rows > 0) {
+        if (L.ring_slot >= 0 && L.num_rows > 0) {
             grg_b200_ring* r = a->ring;
-            if (used[L.slot]) GRG_CUDA_TRY(cudaStreamWaitEvent(r->copy, r->free_ev[L.slot], 0));
-            GRG_CUDA_TRY(cudaMemcpyAsync(a->slot_buffers[L.slot], L.blob, static_cast<size_t>(L.blob_bytes), cudaMemcpyHostToDevice, r->copy));
-            GRG_CUDA_TRY(cudaEventRecord(r->ready[L.slot], r->copy));
-            GRG_CUDA_TRY(cudaStreamWaitEvent(s, r->ready[L.slot], 0));
-            blob = a->slot_buffers[L.slot];
+            if (used[L.ring_slot]) GRG_CUDA_TRY(cudaStreamWaitEvent(r->copy, r->free_ev[L.ring_slot], 0));
+            GRG_CUDA_TRY(cudaMemcpyAsync(a->slot_buffers[L.ring_slot], L.blob, static_cast<size_t>(L.blob_bytes), cudaMemcpyHostToDevice, r->copy));
+            GRG_CUDA_TRY(cudaEventRecord(r->ready[L.ring_slot], r->copy));
+            GRG_CUDA_TRY(cudaStreamWaitEvent(s, r->ready[L.ring_slot], 0));
+            blob = a->slot_buffers[L.ring_slot];
         }
         rc = run_level(a, sh, &L, blob, s);
         if (rc) return rc;
-        if (L.slot >= 0 && L.num_rows > 0) {
-            GRG_CUDA_TRY(cudaEventRecord(a->ring->free_ev[L.slot], s));
-            used[L.slot] = true;
+        if (L.ring_slot >= 0 && L.num_rows > 0) {
+            GRG_CUDA_TRY(cudaEventRecord(a->ring->free_ev[L.ring_slot], s));
+            used[L.ring_slot] = true;
         }
     }
     if (any_streamed) {

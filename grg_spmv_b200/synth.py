@@ -38,7 +38,8 @@ class SynthSpec:
     num_nodes: int  # target total node count, samples included
     num_mutations: int
     children: tuple[int, int] = (2, 8)
-    neighbor_scale: float = 0.5
+    neighbor_scale: float = 0.08  # abutting children are at most ~this fraction of the anchor
+    prefer_largest: float = 0.7  # probability of taking the longest fitting neighbor
     level_decay: float = 1.0
     miss_fraction: float = 0.0
     ploidy: int = 1
@@ -50,7 +51,7 @@ class SynthSpec:
 # Shapes of the benchmark configurations (see DESIGN.md for the measured N/E of each).
 CONFIG1 = SynthSpec(num_samples=2_000, num_levels=16, num_nodes=80_000, num_mutations=20_000, children=(2, 8), seed=0)
 CONFIG2 = SynthSpec(num_samples=100_000, num_levels=40, num_nodes=5_000_000, num_mutations=1_000_000,
-                    children=(2, 28), miss_fraction=0.01, seed=0)
+                    children=(2, 22), miss_fraction=0.01, seed=0)
 
 
 def _level_sizes(spec: SynthSpec) -> np.ndarray:
@@ -87,12 +88,15 @@ class _IntervalIndex:
         out[order] = np.searchsorted(self.key, needles[order], side=side)
         return out
 
-    def pick(self, rng, bound: np.ndarray, cap: np.ndarray) -> np.ndarray:
+    def pick(self, rng, bound: np.ndarray, cap: np.ndarray, largest: float) -> np.ndarray:
+        """An abutting node no longer than ``cap``: with probability ``largest`` the longest
+        such node (which tends to come from a recent level), otherwise a uniform one."""
         base = bound.astype(np.int64) * self.span
         lo = self._search(base + 1, "left")
         hi = self._search(base + cap.astype(np.int64), "right")
         hi = np.maximum(hi, lo + 1)  # the single-sample node (length 1) always qualifies
-        return self.ids[lo + (rng.random(lo.size) * (hi - lo)).astype(np.int64)]
+        uniform = lo + (rng.random(lo.size) * (hi - lo)).astype(np.int64)
+        return self.ids[np.where(rng.random(lo.size) < largest, hi - 1, uniform)]
 
 
 def generate_dag(spec: SynthSpec) -> DagGRG:
@@ -133,11 +137,11 @@ def generate_dag(spec: SynthSpec) -> DagGRG:
             right = idx[go_right]
             left = idx[~go_right]
             if right.size:
-                pick = by_start.pick(rng, b[right], cap[go_right])
+                pick = by_start.pick(rng, b[right], cap[go_right], spec.prefer_largest)
                 kids[right, step] = pick
                 b[right] = all_end[pick]
             if left.size:
-                pick = by_end.pick(rng, a[left], cap[~go_right])
+                pick = by_end.pick(rng, a[left], cap[~go_right], spec.prefer_largest)
                 kids[left, step] = pick
                 a[left] = all_start[pick]
         # Order the level's nodes by interval start for positional locality.

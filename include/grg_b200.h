@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 1
+#define GRG_B200_ABI_VERSION 3
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -89,14 +89,17 @@ typedef enum grg_b200_bias {
 #define GRG_B200_MAX_ID 0x1FFFFFFFu
 
 /*
- * One destination level.  Its gather structure is one byte blob with three arrays at
- * 16-byte aligned offsets:
- *   int32  row_ptr[num_rows + 1]     entry offsets of each row
- *   int32  heavy_rows[num_heavy]     level-local rows with more than heavy_threshold
- *                                    entries (processed one CTA per row)
+ * One destination level.  Its gather structure is one byte blob with these arrays at
+ * 16-byte aligned offsets.  Rows are stored in *processing order* (chosen on the host for
+ * cache locality); processing position p computes level-local row row_ids[p] (or p itself
+ * when off_row_ids < 0).  Rows with more than heavy_threshold entries are the last num_heavy
+ * positions (processed one CTA per row); narrow kernels cover the first num_rows - num_heavy:
+ *   int32  row_ptr[num_rows + 1]     entry offsets of each processing position
+ *   int32  heavy_rows[num_heavy]     the heavy positions (num_rows - num_heavy, ...)
+ *   int32  row_ids[num_rows]         optional processing position -> level-local row
  *   uint32 entries[num_entries]
- * slot < 0: blob is device memory.  slot >= 0: blob is pinned host memory that
- * grg_b200_traverse copies into ring slot `slot` before the level runs.
+ * ring_slot < 0: blob is device memory.  ring_slot >= 0: blob is pinned host memory that
+ * grg_b200_traverse copies into ring slot `ring_slot` before the level runs.
  */
 typedef struct grg_b200_level {
     int64_t row_begin;
@@ -104,11 +107,12 @@ typedef struct grg_b200_level {
     int64_t num_entries;
     int64_t num_heavy;
     int32_t heavy_threshold;
-    int32_t slot;
+    int32_t ring_slot;
     const void* blob;
     int64_t blob_bytes;
     int64_t off_row_ptr;
     int64_t off_heavy;
+    int64_t off_row_ids; /* -1: identity order */
     int64_t off_entries;
 } grg_b200_level;
 
@@ -158,7 +162,14 @@ typedef struct grg_b200_traverse_args {
     const int64_t* slot_bytes;
     int32_t num_slots;
     int32_t* error_word;                /* optional device int32: first failed bounds check */
+    int32_t narrow_variant;             /* narrow-row kernel shape, 0..GRG_B200_NARROW_VARIANTS-1:
+                                           0: 4 rows per round; 1: 8 rows per round; 2: 4 rows per
+                                           round from a shared-memory staged list; 3: 16 rows per
+                                           round, staged; 4: cp.async gathers into shared memory,
+                                           then in-order sums.  Chosen by the runtime's autotuner. */
 } grg_b200_traverse_args;
+
+#define GRG_B200_NARROW_VARIANTS 5
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

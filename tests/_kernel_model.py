@@ -14,10 +14,10 @@ from grg_spmv_b200.backends.b200 import _native as nat
 from grg_spmv_b200.backends.b200.structures import build_down_levels, build_up_levels, load_blocks
 
 
-def _row_sum(lv, r, state, x, miss, acc):
+def _row_sum(codes, state, x, miss, acc):
     seg = np.zeros_like(acc)
-    for e in range(int(lv.row_ptr[r]), int(lv.row_ptr[r + 1])):
-        code = int(lv.entries[e])
+    for code in codes:
+        code = int(code)
         if code & nat.SEG_START:
             acc = acc + seg
             seg = np.zeros_like(acc)
@@ -59,16 +59,16 @@ def model_matmul(path, x, direction, dtype=np.float64, *, init=None, miss=None, 
             if r < st.num_samples:
                 v = v + xi[s2i[r] if by_individual else r]
             state[r] = v
-        for lv in build_up_levels(off, coo, 1 << 30):
-            for r in range(lv.num_rows):
-                state[lv.row_begin + r] = _row_sum(lv, r, state, xi, None, init_row(lv.row_begin + r))
+        for lv in build_up_levels(off, coo, 1 << 30, locality=True):
+            for r, codes in lv.row_lists():
+                state[lv.row_begin + r] = _row_sum(codes, state, xi, None, init_row(lv.row_begin + r))
     else:
         sel_mut = (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations)
         sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations)
         mi = None if miss is None else np.ascontiguousarray(miss.T.astype(dt))
-        for lv in build_down_levels(off, coo, sel_mut, sel_miss, 1 << 30):
-            for r in range(lv.num_rows):
-                state[lv.row_begin + r] = _row_sum(lv, r, state, xi, mi, init_row(lv.row_begin + r))
+        for lv in build_down_levels(off, coo, sel_mut, sel_miss, 1 << 30, locality=True):
+            for r, codes in lv.row_lists():
+                state[lv.row_begin + r] = _row_sum(codes, state, xi, mi, init_row(lv.row_begin + r))
     if emit_all_nodes:
         return state[np.asarray(st.inv_node_perm)].T
     if direction == "up":

@@ -22,11 +22,14 @@ def _req(k=8, **kw):
     return RuntimeRequirements(**base)
 
 
-def _layout(paths, *, dtype=np.float64, req=None, exact=False, heavy=None, budget=0, ring=0, allow_residency=True, stream=0, pair=None):
+def _layout(paths, *, dtype=np.float64, req=None, exact=False, heavy=None, budget=0, ring=0, allow_residency=True, stream=0,
+            pair=None, variant=0):
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, plan_b200_layout
 
     if pair is None:
-        kw = {} if heavy is None else {"heavy_threshold": heavy}
+        kw = {"narrow_variant": variant}
+        if heavy is not None:
+            kw["heavy_threshold"] = heavy
         pair = B200PlanPair(plan_up=B200Plan(exact_order=exact, **kw), plan_down=B200Plan(exact_order=exact, **kw))
     return plan_b200_layout(artifacts=list(paths), dtype=dtype, requirements=req or _req(), vram_budget_bytes=budget,
                             ring_buffer_size=ring, allow_residency=allow_residency, device=0, stream=stream, pair=pair)
@@ -49,14 +52,16 @@ def _cases_by_artifact():
 GROUPS = _cases_by_artifact()
 
 
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("heavy", [128, 2], ids=["narrow", "heavy-rows"])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
-def test_golden_bit_exact_in_exact_order(group, heavy, golden_data):
-    """exact_order=True reproduces ReferenceRuntime bit for bit, for every golden case."""
+def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
+    """exact_order=True reproduces ReferenceRuntime bit for bit, for every golden case and
+    every narrow-row kernel variant."""
     from grg_spmv_b200.backends.b200 import B200Runtime
 
     name, dtype = group
-    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=True, heavy=heavy)
+    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=True, heavy=heavy, variant=variant)
     with B200Runtime(layout, check_bounds=True) as runtime:
         (grg,) = runtime.grgs
         for case in GROUPS[group]:

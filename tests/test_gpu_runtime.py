@@ -1,0 +1,333 @@
+"""B200 runtime contracts (the reference suite's Triton/cuSPARSE runtime tests, restated)."""
+
+from __future__ import annotations
+
+from contextlib import ExitStack
+import warnings
+
+import numpy as np
+import pytest
+
+from conftest import artifact_path
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+from grg_spmv_b200 import RuntimeRequirements  # noqa: E402
+from grg_oracle import OracleGRG  # noqa: E402
+
+
+def _req(k=2, **kw):
+    base = dict(max_k_up=k, max_k_down=k, need_down_miss_input=True, need_up_miss_output=True, need_init_vector=True,
+                need_init_matrix=True, need_init_xtx=True)
+    base.update(kw)
+    return RuntimeRequirements(**base)
+
+
+def _layout(paths, **kw):
+    from grg_spmv_b200.backends.b200 import plan_b200_layout
+
+    kw.setdefault("dtype", np.float64)
+    kw.setdefault("requirements", _req())
+    kw.setdefault("vram_budget_bytes", 0)
+    kw.setdefault("ring_buffer_size", 0)
+    kw.setdefault("device", 0)
+    kw.setdefault("stream", 0)
+    return plan_b200_layout(artifacts=[str(p) for p in paths], **kw)
+
+
+def _runtime(layout, **kw):
+    from grg_spmv_b200.backends.b200 import B200Runtime
+
+    return B200Runtime(layout, check_bounds=True, **kw)
+
+
+def _pm1(rng, shape):
+    return rng.choice(np.asarray([-1.0, 1.0]), size=shape)
+
+
+@pytest.fixture(scope="module")
+def synth_artifact(tmp_path_factory):
+    from grg_spmv_b200.synth import SynthSpec, write_synthetic_artifact
+
+    path = tmp_path_factory.mktemp("synth") / "mid.grg_spmv"
+    write_synthetic_artifact(SynthSpec(num_samples=3000, num_levels=14, num_nodes=60_000, num_mutations=15_000, children=(2, 16),
+                                       miss_fraction=0.02, ploidy=2, with_coalescence=True, random_ids=True, seed=21), path)
+    return path
+
+
+def test_runtime_requires_enter_and_exposes_stream():
+    stream = torch.cuda.Stream(device=0)
+    layout = _layout([artifact_path("band3")], stream=stream)
+    runtime = _runtime(layout)
+    with pytest.raises(RuntimeError, match="entered"):
+        _ = runtime.grgs
+    with runtime:
+        assert runtime.stream_ptr == int(stream.cuda_stream) == int(runtime.stream.cuda_stream)
+        assert len(runtime.grgs) == 1 and runtime.grgs[0].device == 0
+    assert runtime._state is None and not runtime._entered
+
+
+def test_enter_failure_releases_owned_state(monkeypatch):
+    from grg_spmv_b200.backends.b200 import B200Runtime
+
+    layout = _layout([artifact_path("band3")])
+    runtime = _runtime(layout)
+
+    def boom(self, art):
+        raise RuntimeError("boom")
+
+    monkeypatch.setattr(B200Runtime, "_build_artifact", boom)
+    with pytest.raises(RuntimeError, match="boom"):
+        runtime.__enter__()
+    assert runtime._state is None and runtime._io0 is None and runtime._artifacts == () and not runtime._entered
+
+
+def test_concurrent_calls_fail_fast():
+    with _runtime(_layout([artifact_path("band3")])) as runtime:
+        (grg,) = runtime.grgs
+        with grg.prepare_matmul_cuda(direction="up", k=1) as op:
+            with runtime._call_scope():
+                with pytest.raises(RuntimeError, match="concurrent"):
+                    op()
+
+
+def test_up_output_aliases_down_input():
+    with _runtime(_layout([artifact_path("band3")])) as runtime:
+        (grg,) = runtime.grgs
+        up = grg.prepare_matmul_cuda(direction="up", k=2)
+        down = grg.prepare_matmul_cuda(direction="down", k=2)
+        assert up.output.data_ptr() == down.input.data_ptr()
+        assert up.input.shape == (2, grg.num_samples) and up.output.shape == (2, grg.num_mutations)
+
+
+@pytest.mark.parametrize("k", [1, 2, 3, 5, 8, 16, 33])
+@pytest.mark.parametrize("variant", [0, 4])
+def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
+    """Integer-valued inputs are exact; real-valued inputs agree to 1e-12 (default heavy-row
+    reduction) — every mode of the hot path on a 60k-node graph with random node ids."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    oracle = OracleGRG(synth_artifact)
+    pair = B200PlanPair(plan_up=B200Plan(narrow_variant=variant, heavy_threshold=24),
+                        plan_down=B200Plan(narrow_variant=variant, heavy_threshold=24))
+    rng = np.random.default_rng(100 + k)
+    with _runtime(_layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=pair)) as runtime:
+        (grg,) = runtime.grgs
+        S, M, N, I = grg.num_samples, grg.num_mutations, grg.num_nodes, grg.num_individuals
+        for direction, cols in (("up", S), ("down", M)):
+            x = _pm1(rng, (k, cols))
+            np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
+            x = rng.standard_normal((k, cols))
+            np.testing.assert_allclose(grg.matmul(x, direction), oracle.matmul(x, direction), rtol=1e-12, atol=1e-9)
+            init = rng.standard_normal(k)
+            np.testing.assert_allclose(grg.matmul(x, direction, init=init), oracle.matmul(x, direction, init=init),
+                                       rtol=1e-12, atol=1e-9)
+            np.testing.assert_allclose(grg.matmul(x, direction, init="xtx"), oracle.matmul(x, direction, init="xtx"),
+                                       rtol=1e-12, atol=1e-9)
+            mat = rng.standard_normal((k, N))
+            np.testing.assert_allclose(grg.matmul(x, direction, init=mat, emit_all_nodes=True),
+                                       oracle.matmul(x, direction, init=mat, emit_all_nodes=True), rtol=1e-12, atol=1e-9)
+        xi = _pm1(rng, (k, I))
+        miss_b, miss_o = np.zeros((k, M)), np.zeros((k, M))
+        np.testing.assert_array_equal(grg.matmul(xi, "up", by_individual=True, miss=miss_b),
+                                      oracle.matmul(xi, "up", by_individual=True, miss=miss_o))
+        np.testing.assert_array_equal(miss_b, miss_o)
+        xd, miss = _pm1(rng, (k, M)), _pm1(rng, (k, M))
+        np.testing.assert_array_equal(grg.matmul(xd, "down", by_individual=True, miss=miss.copy()),
+                                      oracle.matmul(xd, "down", by_individual=True, miss=miss.copy()))
+        assert runtime.device_error() == 0
+
+
+def test_float32_runtime(synth_artifact):
+    oracle = OracleGRG(synth_artifact, dtype=np.float32)
+    rng = np.random.default_rng(7)
+    with _runtime(_layout([synth_artifact], dtype=np.float32, requirements=_req(k=4))) as runtime:
+        (grg,) = runtime.grgs
+        for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
+            x = _pm1(rng, (4, cols)).astype(np.float32)
+            out = grg.matmul(x, direction)
+            assert out.dtype == np.float32
+            np.testing.assert_array_equal(out, oracle.matmul(x, direction))
+            x = rng.standard_normal((4, cols)).astype(np.float32)
+            np.testing.assert_allclose(grg.matmul(x, direction), oracle.matmul(x, direction), rtol=2e-5, atol=1e-4)
+
+
+def test_repeated_calls_are_deterministic(synth_artifact):
+    rng = np.random.default_rng(8)
+    with _runtime(_layout([synth_artifact], requirements=_req(k=4))) as runtime:
+        (grg,) = runtime.grgs
+        x = rng.standard_normal((4, grg.num_mutations))
+        first = grg.matmul(x, "down")
+        for _ in range(3):
+            np.testing.assert_array_equal(grg.matmul(x, "down"), first)
+
+
+@pytest.mark.parametrize("ring", [1, 2, 3])
+def test_streamed_levels_are_exact(synth_artifact, ring):
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(30 + ring)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        layout = _layout([synth_artifact], requirements=_req(k=3), ring_buffer_size=ring, allow_residency=False)
+    assert layout.allocated_ring_buffer_size == ring
+    assert layout.bytes_by_category["resident_sparse"] == 0
+    with _runtime(layout) as runtime:
+        (grg,) = runtime.grgs
+        for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
+            x = _pm1(rng, (3, cols))
+            np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
+
+
+def test_hybrid_budget_is_exact(synth_artifact):
+    oracle = OracleGRG(synth_artifact)
+    full = _layout([synth_artifact], requirements=_req(k=2))
+    sizes = sorted((lp.nbytes for lp in full.level_plans()), reverse=True)
+    fixed = full.bytes_total - full.bytes_by_category["resident_sparse"]
+    budget = fixed + 2 * sizes[0] + sum(sizes[1:4])
+    layout = _layout([synth_artifact], requirements=_req(k=2), vram_budget_bytes=budget, ring_buffer_size=2)
+    resident = [lp for lp in layout.level_plans() if lp.resident]
+    streamed = [lp for lp in layout.level_plans() if not lp.resident]
+    assert resident and streamed and layout.bytes_total <= budget
+    rng = np.random.default_rng(5)
+    with _runtime(layout) as runtime:
+        (grg,) = runtime.grgs
+        used = sum(t.numel() * t.element_size() for t in (runtime._state, runtime._io0, runtime._io1, runtime._aux)) + sum(
+            s.numel() for s in runtime._slots)
+        assert used <= budget
+        for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
+            x = _pm1(rng, (2, cols))
+            np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
+
+
+def test_one_sided_layouts(synth_artifact):
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(9)
+    for direction in ("up", "down"):
+        pair = B200PlanPair(plan_up=B200Plan() if direction == "up" else None, plan_down=B200Plan() if direction == "down" else None)
+        with _runtime(_layout([synth_artifact], requirements=_req(k=4), pair=pair)) as runtime:
+            (grg,) = runtime.grgs
+            cols = grg.num_samples if direction == "up" else grg.num_mutations
+            x = _pm1(rng, (4, cols))
+            np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
+            other = "down" if direction == "up" else "up"
+            with pytest.raises(ValueError, match="not configured"):
+                grg.prepare_matmul_cuda(direction=other, k=1)
+
+
+@pytest.mark.parametrize("direction", ["up", "down"])
+def test_k_below_max_with_matrix_and_emit_vector(synth_artifact, direction):
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(10)
+    with _runtime(_layout([synth_artifact], requirements=_req(k=4))) as runtime:
+        (grg,) = runtime.grgs
+        cols = grg.num_samples if direction == "up" else grg.num_mutations
+        x = rng.standard_normal((2, cols))
+        init = rng.standard_normal((2, grg.num_nodes))
+        np.testing.assert_allclose(grg.matmul(x, direction, init=init), oracle.matmul(x, direction, init=init), rtol=1e-12, atol=1e-9)
+        x1 = rng.standard_normal((1, cols))
+        v = rng.standard_normal(1)
+        np.testing.assert_allclose(grg.matmul(x1, direction, init=v, emit_all_nodes=True),
+                                   oracle.matmul(x1, direction, init=v, emit_all_nodes=True), rtol=1e-12, atol=1e-9)
+
+
+def _chain_expected(oracle, order, src, init_first, init_second):
+    mid = oracle.matmul(src, order[0], init=init_first)
+    return oracle.matmul(mid, order[1], init=init_second)
+
+
+@pytest.mark.parametrize("streamed", [False, True], ids=["resident", "streamed"])
+def test_prepared_chain_captures_in_a_cuda_graph(synth_artifact, streamed):
+    """down -> up with vector init, captured by the caller in one CUDA graph and replayed."""
+    oracle = OracleGRG(synth_artifact)
+    capture_stream = torch.cuda.Stream(device=0)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)
+        layout = _layout([synth_artifact], requirements=_req(k=2), stream=capture_stream, ring_buffer_size=2 if streamed else 0,
+                         allow_residency=not streamed)
+    rng = np.random.default_rng(98)
+    order = ("down", "up")
+    src_np = rng.standard_normal((2, oracle.num_mutations))
+    i1, i2 = rng.standard_normal(2), rng.standard_normal(2)
+    expected = _chain_expected(oracle, order, src_np, i1, i2)
+    with _runtime(layout) as runtime, ExitStack() as stack:
+        (grg,) = runtime.grgs
+        first = stack.enter_context(grg.prepare_matmul_cuda(direction=order[0], k=2, init_mode="vector"))
+        second = stack.enter_context(grg.prepare_matmul_cuda(direction=order[1], k=2, init_mode="vector"))
+        assert first.output.data_ptr() == second.input.data_ptr()
+        src = torch.from_numpy(src_np).to("cuda:0")
+        t1, t2 = torch.from_numpy(i1).to("cuda:0"), torch.from_numpy(i2).to("cuda:0")
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=capture_stream):
+            first.input.copy_(src)
+            first.init_vector.copy_(t1)
+            first()
+            second.init_vector.copy_(t2)
+            second()
+        for _ in range(2):
+            graph.replay()
+            torch.cuda.synchronize()
+            np.testing.assert_allclose(second.output.cpu().numpy(), expected, rtol=1e-12, atol=1e-6)
+
+
+def test_multi_grg_single_graph_mixed_heights():
+    oracle_tall, oracle_short = OracleGRG(artifact_path("overlap4")), OracleGRG(artifact_path("band3"))
+    capture_stream = torch.cuda.Stream(device=0)
+    layout = _layout([artifact_path("overlap4"), artifact_path("band3")], requirements=_req(k=1), stream=capture_stream)
+    cases = []
+    for idx, (oracle, order) in enumerate(((oracle_tall, ("up", "down")), (oracle_short, ("down", "up")))):
+        cols = oracle.num_samples if order[0] == "up" else oracle.num_mutations
+        src = np.arange(cols, dtype=np.float64).reshape(1, cols) + 100.0 * idx
+        i1, i2 = np.asarray([0.25 + idx]), np.asarray([0.75 + idx])
+        cases.append((order, src, i1, i2, _chain_expected(oracle, order, src, i1, i2)))
+    with _runtime(layout) as runtime, ExitStack() as stack:
+        results, ops = [], []
+        for grg, (order, src, i1, i2, _) in zip(runtime.grgs, cases):
+            a = stack.enter_context(grg.prepare_matmul_cuda(direction=order[0], k=1, init_mode="vector"))
+            b = stack.enter_context(grg.prepare_matmul_cuda(direction=order[1], k=1, init_mode="vector"))
+            ops.append((a, b, torch.from_numpy(src).to("cuda:0"), torch.from_numpy(i1).to("cuda:0"), torch.from_numpy(i2).to("cuda:0")))
+            results.append(torch.empty_like(b.output))
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=capture_stream):
+            for (a, b, src, i1, i2), res in zip(ops, results):
+                a.input.copy_(src)
+                a.init_vector.copy_(i1)
+                a()
+                b.init_vector.copy_(i2)
+                b()
+                res.copy_(b.output)
+        graph.replay()
+        torch.cuda.synchronize()
+        for res, case in zip(results, cases):
+            np.testing.assert_allclose(res.cpu().numpy(), case[4], rtol=1e-12, atol=1e-9)
+
+
+def test_graphs_off_matches_graphs_on(synth_artifact):
+    rng = np.random.default_rng(11)
+    outs = []
+    for use_graphs in (True, False):
+        with _runtime(_layout([synth_artifact], requirements=_req(k=3)), use_graphs=use_graphs) as runtime:
+            (grg,) = runtime.grgs
+            x = np.asarray(rng.standard_normal((3, grg.num_mutations))) if not outs else outs[0][0]
+            outs.append((x, grg.matmul(x, "down")))
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+
+
+def test_foreign_stream_ordering(synth_artifact):
+    """Work queued on the caller's stream before a call is seen by it; the result is ready for
+    work queued after it on the same stream."""
+    oracle = OracleGRG(synth_artifact)
+    stream = torch.cuda.Stream(device=0)
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((2, oracle.num_samples))
+    with _runtime(_layout([synth_artifact], requirements=_req(k=2), stream=stream)) as runtime:
+        (grg,) = runtime.grgs
+        with grg.prepare_matmul_cuda(direction="up", k=2) as op, torch.cuda.stream(stream):
+            torch.cuda._sleep(2_000_000)
+            op.input.copy_(torch.from_numpy(x).to("cuda:0"))
+            op()
+            out = op.output.clone()
+        stream.synchronize()
+        np.testing.assert_allclose(out.cpu().numpy(), oracle.matmul(x, "up"), rtol=1e-12, atol=1e-9)
