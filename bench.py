@@ -61,6 +61,7 @@ def parse_args():
     p.add_argument("--heavy-threshold", type=int, default=None)
     p.add_argument("--variant", type=int, default=None, help="narrow-row kernel variant")
     p.add_argument("--no-graphs", action="store_true", help="launch kernels per level instead of replaying a CUDA graph")
+    p.add_argument("--no-balance", action="store_true", help="do not group narrow rows by length")
     p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
     p.add_argument("--row-order-down", choices=["natural", "locality"], default=None)
     return p.parse_args()
@@ -188,6 +189,8 @@ def run_b200(args) -> None:
     extra = {} if args.heavy_threshold is None else {"heavy_threshold": args.heavy_threshold}
     if args.variant is not None:
         extra["narrow_variant"] = args.variant
+    if args.no_balance:
+        extra["balance"] = False
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
                         plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
     stream = torch.cuda.Stream(device=device)
@@ -259,8 +262,12 @@ def run_b200(args) -> None:
     level_ms = {"up": 0.0, "down": 0.0}
     level_launches = 0
     lv_bytes = 0
+    all_evs = []
     with torch.cuda.device(device), torch.cuda.stream(stream):
         up.input.copy_(x_up)
+        # Hold the stream for ~50 ms so the host enqueues every launch and event before the
+        # GPU reaches them: event deltas then time kernels, not host launch latency.
+        torch.cuda._sleep(100_000_000)
         for name, op in (("up", up), ("down", down)):
             args_c = op._args
             if name == "up":
@@ -279,14 +286,16 @@ def run_b200(args) -> None:
                 nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
             else:
                 nat.check(lib, lib.grg_b200_output_down(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_down")
-            torch.cuda.synchronize(device)
+            all_evs.append((name, evs, list(levels.array)))
+        torch.cuda.synchronize(device)
+        for name, evs, lvs in all_evs:
             level_ms[name] = sum(a.elapsed_time(b) for a, b in evs)
-            for (a, b), lv in zip(evs, list(levels.array)):
+            for (a, b), lv in zip(evs, lvs):
                 ms = a.elapsed_time(b)
                 nbytes = level_bytes([lv], k, 8, "up", M, False)
                 print(f"[level] {name} rows={lv.num_rows} entries={lv.num_entries} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
-            lv_bytes += level_bytes(list(levels.array), k, 8, name, M, use_miss=True)
+            lv_bytes += level_bytes(lvs, k, 8, name, M, use_miss=True)
     launches_per_step = level_launches + 1 + 1 + 1  # + seed_up + output_up + output_down
     level_total_ms = level_ms["up"] + level_ms["down"]
     peak, peak_kind = measured_peak_hbm()
@@ -369,7 +378,7 @@ def run_b200(args) -> None:
                        "k": k, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": pair.plan_down.narrow_variant,
-                       "cuda_graphs": not args.no_graphs,
+                       "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
                        "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},

@@ -36,7 +36,7 @@ SRC_SHIFT = 29
 SRC_STATE, SRC_INPUT, SRC_MISS = 0, 1, 2
 ID_MASK = 0x1FFFFFFF
 MAX_ID = 0x1FFFFFFF
-NARROW_VARIANTS = 5
+NARROW_VARIANTS = 6
 
 
 class Level(ctypes.Structure):

@@ -34,7 +34,7 @@ from grg_spmv_b200.artifact import ArtifactScan, scan_grg_spmv
 from grg_spmv_b200.backends.b200.structures import blob_layout, down_entry_bound, up_entry_bound
 from grg_spmv_b200.types import Direction
 
-DEFAULT_HEAVY_THRESHOLD = 128
+DEFAULT_HEAVY_THRESHOLD = 32
 
 
 @dataclass(frozen=True)
@@ -60,20 +60,23 @@ class B200Plan:
     ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
     processed together); None picks the direction's default (up natural, down locality).
     ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``).
+    ``balance``: group narrow rows by length (power-of-two buckets) so a warp's rows finish
+    together.
     """
 
     exact_order: bool = False
     heavy_threshold: int = DEFAULT_HEAVY_THRESHOLD
     row_order: str | None = None
-    narrow_variant: int = 0
+    narrow_variant: int = 5
+    balance: bool = True
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
         if self.row_order not in (None, "natural", "locality"):
             raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
-        if not 0 <= int(self.narrow_variant) < 5:
-            raise ValueError(f"narrow_variant must be in [0, 5), got {self.narrow_variant}")
+        if not 0 <= int(self.narrow_variant) < 6:
+            raise ValueError(f"narrow_variant must be in [0, 6), got {self.narrow_variant}")
 
     def locality(self, direction: Direction) -> bool:
         if self.row_order is None:
@@ -82,13 +85,14 @@ class B200Plan:
 
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
-        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant"}
+        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
         return cls(exact_order=bool(value.get("exact_order", False)),
                    heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)),
-                   row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 0)))
+                   row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 5)),
+                   balance=bool(value.get("balance", True)))
 
 
 @dataclass(frozen=True)

@@ -232,8 +232,8 @@ __device__ __forceinline__ int64_t level_row(const LevelArgs& a, int64_t pos) {
 // restarting the partial sum at every segment start.
 //
 // Variants (``narrow_variant``): U = rows fetched per round, STAGE = shared-memory staging.
-template <typename T, int V, int INIT, int U, bool STAGE>
-__global__ void __launch_bounds__(kNarrowThreads) level_narrow_kernel(LevelArgs a) {
+template <typename T, int V, int INIT, int U, bool STAGE, int MIN_BLOCKS = 1>
+__global__ void __launch_bounds__(kNarrowThreads, MIN_BLOCKS) level_narrow_kernel(LevelArgs a) {
     __shared__ uint32_t stage[kNarrowWarps][STAGE ? kStageCap : 1];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -707,19 +707,20 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     } else if (narrow > 0) {
         const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
-#define GRG_NARROW(INIT, U, ST) level_narrow_kernel<T, V, INIT, U, ST><<<grid, kNarrowThreads, 0, s>>>(la)
-#define GRG_NARROW_INIT(U, ST)                  \
-    switch (init_mode) {                        \
-        case 0: GRG_NARROW(0, U, ST); break;    \
-        case 1: GRG_NARROW(1, U, ST); break;    \
-        case 2: GRG_NARROW(2, U, ST); break;    \
-        default: GRG_NARROW(3, U, ST); break;   \
+#define GRG_NARROW(INIT, U, ST, MB) level_narrow_kernel<T, V, INIT, U, ST, MB><<<grid, kNarrowThreads, 0, s>>>(la)
+#define GRG_NARROW_INIT(U, ST, MB)                  \
+    switch (init_mode) {                            \
+        case 0: GRG_NARROW(0, U, ST, MB); break;    \
+        case 1: GRG_NARROW(1, U, ST, MB); break;    \
+        case 2: GRG_NARROW(2, U, ST, MB); break;    \
+        default: GRG_NARROW(3, U, ST, MB); break;   \
     }
         switch (variant) {
-            case 1: GRG_NARROW_INIT(8, false) break;
-            case 2: GRG_NARROW_INIT(4, true) break;
-            case 3: GRG_NARROW_INIT(16, true) break;
-            default: GRG_NARROW_INIT(4, false) break;
+            case 1: GRG_NARROW_INIT(8, false, 1) break;
+            case 2: GRG_NARROW_INIT(4, true, 1) break;
+            case 3: GRG_NARROW_INIT(16, true, 1) break;
+            case 5: GRG_NARROW_INIT(4, false, 8) break;
+            default: GRG_NARROW_INIT(4, false, 1) break;
         }
 #undef GRG_NARROW_INIT
 #undef GRG_NARROW

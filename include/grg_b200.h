@@ -166,10 +166,11 @@ typedef struct grg_b200_traverse_args {
                                            0: 4 rows per round; 1: 8 rows per round; 2: 4 rows per
                                            round from a shared-memory staged list; 3: 16 rows per
                                            round, staged; 4: cp.async gathers into shared memory,
-                                           then in-order sums.  Chosen by the runtime's autotuner. */
+                                           then in-order sums; 5: as 0 with at most 32 registers
+                                           per thread (8 CTAs per SM). */
 } grg_b200_traverse_args;
 
-#define GRG_B200_NARROW_VARIANTS 5
+#define GRG_B200_NARROW_VARIANTS 6
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);
