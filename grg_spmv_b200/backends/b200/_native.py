@@ -116,6 +116,7 @@ EXPORTED_SYMBOLS = (
     "grg_b200_output_down",
     "grg_b200_emit_all",
     "grg_b200_traverse",
+    "grg_b200_traverse_static",
 )
 
 _lock = threading.Lock()
@@ -156,7 +157,8 @@ def load_library():
         lib.grg_b200_last_error.restype = ctypes.c_size_t
         lib.grg_b200_ring_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
         lib.grg_b200_ring_destroy.argtypes = [ctypes.c_void_p]
-        for name in ("grg_b200_seed_up", "grg_b200_output_up", "grg_b200_output_down", "grg_b200_emit_all", "grg_b200_traverse"):
+        for name in ("grg_b200_seed_up", "grg_b200_output_up", "grg_b200_output_down", "grg_b200_emit_all", "grg_b200_traverse",
+                     "grg_b200_traverse_static"):
             getattr(lib, name).argtypes = [ctypes.POINTER(TraverseArgs), ctypes.c_void_p]
             getattr(lib, name).restype = ctypes.c_int
         lib.grg_b200_run_level.argtypes = [ctypes.POINTER(TraverseArgs), ctypes.POINTER(Level), ctypes.c_void_p]

@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 
 #include "grg_b200.h"
@@ -1047,6 +1048,69 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
     if (a->emit_all_nodes) return emit_all_impl(a, sh, s);
     if (a->direction == GRG_B200_UP) return output_up_impl(a, sh, s);
     return output_down_impl(a, sh, s);
+}
+
+// ---------------------------------------------------------------------------------------
+// Allocation-free traversal: the node state lives in a fixed device array of this library.
+//
+// Some callers cannot allocate device memory: C/FFI hosts with no device allocator of their
+// own, plugins running inside another framework's memory manager, and code that must not
+// allocate while a stream is being captured.  grg_b200_traverse_static serves them: it takes
+// the same arguments as grg_b200_traverse (inputs, outputs and resident level blobs all come
+// from the caller) but ignores args->state/ld_state and keeps the traversal's node state in
+// g_static_state below.  That array holds GRG_B200_STATIC_STATE_BYTES on every GPU whose
+// context loads this library, for the lifetime of the process.
+// ---------------------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_static_state[GRG_B200_STATIC_STATE_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mutex;
+void* g_static_ptr[kMaxDevices] = {};
+
+// Device address of g_static_state on the current device; looked up once per device (the
+// host symbol g_static_state is only a stand-in and must never reach a kernel).
+int static_state_address(void** out) {
+    int device = 0;
+    GRG_CUDA_TRY(cudaGetDevice(&device));
+    if (device < 0 || device >= kMaxDevices) return fail(GRG_B200_ERR_UNSUPPORTED, "device ordinal %d above %d", device, kMaxDevices);
+    std::lock_guard<std::mutex> lock(g_static_mutex);
+    if (!g_static_ptr[device]) {
+        void* ptr = nullptr;
+        const cudaError_t err = cudaGetSymbolAddress(&ptr, g_static_state);
+        if (err != cudaSuccess || !ptr)
+            return fail(GRG_B200_ERR_CUDA, "cudaGetSymbolAddress(g_static_state) on device %d failed: %s", device,
+                        cudaGetErrorString(err));
+        g_static_ptr[device] = ptr;
+    }
+    *out = g_static_ptr[device];
+    return GRG_B200_OK;
+}
+}  // namespace
+
+int grg_b200_traverse_static(const grg_b200_traverse_args* a, void* stream_handle) {
+    if (!a) return fail(GRG_B200_ERR_INVALID, "args is NULL");
+    if (a->k < 1) return fail(GRG_B200_ERR_INVALID, "k must be >= 1, got %lld", (long long)a->k);
+    const int64_t esize = a->dtype == GRG_B200_F64 ? 8 : 4;
+    if (a->num_nodes < 0 || a->num_nodes > (int64_t)GRG_B200_STATIC_STATE_BYTES / esize / a->k)
+        return fail(GRG_B200_ERR_UNSUPPORTED,
+                    "grg_b200_traverse_static holds at most %lld bytes of node state; %lld nodes x k=%lld need %lld",
+                    (long long)GRG_B200_STATIC_STATE_BYTES, (long long)a->num_nodes, (long long)a->k,
+                    (long long)(a->num_nodes * a->k * esize));
+    for (int i = 0; a->levels && i < a->num_levels; ++i)
+        if (a->levels[i].ring_slot >= 0)
+            return fail(GRG_B200_ERR_UNSUPPORTED, "grg_b200_traverse_static needs every level resident (level %d is streamed)", i);
+    void* state = nullptr;
+    const int rc = static_state_address(&state);
+    if (rc) return rc;
+    grg_b200_traverse_args local = *a;
+    local.state = state;
+    local.ld_state = a->k;
+    local.ring = nullptr;
+    local.slot_buffers = nullptr;
+    local.slot_bytes = nullptr;
+    local.num_slots = 0;
+    return grg_b200_traverse(&local, stream_handle);
 }
 
 }  // extern "C"

@@ -207,6 +207,23 @@ int grg_b200_emit_all(const grg_b200_traverse_args* args, void* stream);
  * the output stage, all on `stream`. */
 int grg_b200_traverse(const grg_b200_traverse_args* args, void* stream);
 
+/* No counterpart in the reference.  The same traversal as grg_b200_traverse for callers that
+ * cannot allocate device memory (C/FFI hosts without a device allocator, plugins inside
+ * another framework's memory manager, code that must not allocate during stream capture):
+ * args->state and args->ld_state are ignored and the node state is kept in a fixed array of
+ * GRG_B200_STATIC_STATE_BYTES inside this library, which every GPU that loads the library
+ * holds until the process exits.  The caller still passes inputs, outputs and level blobs.
+ *   - num_nodes * k * sizeof(element) must not exceed GRG_B200_STATIC_STATE_BYTES, and every
+ *     level must be resident (ring_slot < 0); otherwise GRG_B200_ERR_UNSUPPORTED.
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress,
+ *     once per device, with that device current); make that first call before any stream
+ *     capture that will contain the entry point.
+ *   - All calls share the one array: calls whose work overlaps on the GPU (different streams,
+ *     no ordering between them) race on it.  Calls ordered on one stream are safe; every
+ *     traversal writes each node row before reading it, so nothing needs clearing. */
+#define GRG_B200_STATIC_STATE_BYTES (16u << 20)
+int grg_b200_traverse_static(const grg_b200_traverse_args* args, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
