@@ -62,6 +62,7 @@ def parse_args():
     p.add_argument("--variant", type=int, default=None, help="narrow-row kernel variant")
     p.add_argument("--no-graphs", action="store_true", help="launch kernels per level instead of replaying a CUDA graph")
     p.add_argument("--no-balance", action="store_true", help="do not group narrow rows by length")
+    p.add_argument("--autotune", action="store_true", help="pick the narrow-kernel variant per direction at runtime entry")
     p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
     p.add_argument("--row-order-down", choices=["natural", "locality"], default=None)
     return p.parse_args()
@@ -149,13 +150,22 @@ def measured_peak_hbm() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def level_bytes(levels, k: int, itemsize: int, direction: str, num_mutations: int, use_miss: bool) -> int:
+def level_units(scan, direction: str, level: int, use_miss: bool) -> tuple[int, int]:
+    """(rows, gather entries) of one level from the artifact scan (real edges, no padding)."""
+    from grg_spmv_b200.backends.b200.structures import down_entry_bound, up_entry_bound
+
+    rows = int(scan.level_sizes[level])
+    entries = up_entry_bound(scan, level) if direction == "up" else down_entry_bound(scan, level, use_miss)
+    return rows, entries
+
+
+def level_bytes(units, k: int, itemsize: int, direction: str, num_mutations: int, use_miss: bool) -> int:
     """Algorithmic bytes of one traversal's level kernels: each gather entry (4 B) and row
     pointer (4 B) read once, each destination row written once and read once by later levels
     or the output stage (2·k·b), plus (down) the mutation inputs read once."""
     total = 0
-    for lv in levels:
-        total += 4 * int(lv.num_entries) + 4 * (int(lv.num_rows) + 1) + 2 * int(lv.num_rows) * k * itemsize
+    for rows, entries in units:
+        total += 4 * int(entries) + 4 * (int(rows) + 1) + 2 * int(rows) * k * itemsize
     if direction == "down":
         total += num_mutations * k * itemsize * (2 if use_miss else 1)
     return total
@@ -191,6 +201,8 @@ def run_b200(args) -> None:
         extra["narrow_variant"] = args.variant
     if args.no_balance:
         extra["balance"] = False
+    if args.autotune:
+        extra["autotune"] = True
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
                         plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
     stream = torch.cuda.Stream(device=device)
@@ -286,16 +298,18 @@ def run_b200(args) -> None:
                 nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
             else:
                 nat.check(lib, lib.grg_b200_output_down(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_down")
-            all_evs.append((name, evs, list(levels.array)))
+            lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
+            units = [level_units(scan, name, L, True) for L in lv_order if scan.level_sizes[L] > 0]
+            all_evs.append((name, evs, list(levels.array), units))
         torch.cuda.synchronize(device)
-        for name, evs, lvs in all_evs:
+        for name, evs, lvs, units in all_evs:
             level_ms[name] = sum(a.elapsed_time(b) for a, b in evs)
-            for (a, b), lv in zip(evs, lvs):
+            for (a, b), lv, unit in zip(evs, lvs, units):
                 ms = a.elapsed_time(b)
-                nbytes = level_bytes([lv], k, 8, "up", M, False)
-                print(f"[level] {name} rows={lv.num_rows} entries={lv.num_entries} heavy={lv.num_heavy} "
+                nbytes = level_bytes([unit], k, 8, "up", M, False)
+                print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
-            lv_bytes += level_bytes(lvs, k, 8, name, M, use_miss=True)
+            lv_bytes += level_bytes(units, k, 8, name, M, use_miss=True)
     launches_per_step = level_launches + 1 + 1 + 1  # + seed_up + output_up + output_down
     level_total_ms = level_ms["up"] + level_ms["down"]
     peak, peak_kind = measured_peak_hbm()
@@ -358,6 +372,7 @@ def run_b200(args) -> None:
         rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-300))
         max_rel = max(rel(got_up, ref_up), rel(got_down, ref_down))
 
+    tuned = {d.value: v for d, v in runtime._variant.items()}
     runtime.__exit__(None, None, None)
     if rank == 0:
         line = {
@@ -378,7 +393,8 @@ def run_b200(args) -> None:
                        "k": k, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": pair.plan_down.narrow_variant,
-                       "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance,
+                       "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
+                       "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
                        "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},

@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -33,10 +33,10 @@ INIT_NONE, INIT_VECTOR, INIT_XTX, INIT_MATRIX = 0, 1, 2, 3
 BIAS_NONE, BIAS_VECTOR, BIAS_XTX = 0, 1, 2
 SEG_START = 0x80000000
 SRC_SHIFT = 29
-SRC_STATE, SRC_INPUT, SRC_MISS = 0, 1, 2
+SRC_STATE, SRC_INPUT, SRC_MISS, SRC_NULL = 0, 1, 2, 3
 ID_MASK = 0x1FFFFFFF
 MAX_ID = 0x1FFFFFFF
-NARROW_VARIANTS = 6
+NARROW_VARIANTS = 7
 
 
 class Level(ctypes.Structure):
@@ -53,6 +53,8 @@ class Level(ctypes.Structure):
         ("off_heavy", ctypes.c_int64),
         ("off_row_ids", ctypes.c_int64),
         ("off_entries", ctypes.c_int64),
+        ("list_align", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

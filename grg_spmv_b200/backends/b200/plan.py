@@ -62,21 +62,28 @@ class B200Plan:
     ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``).
     ``balance``: group narrow rows by length (power-of-two buckets) so a warp's rows finish
     together.
+    ``autotune``: time the narrow-kernel variants when the runtime is entered and use the
+    fastest for this direction (instead of ``narrow_variant``).
+    ``pad_lists``: pad every gather list to a multiple of 4 entries (needed by variant 6).
     """
 
     exact_order: bool = False
     heavy_threshold: int = DEFAULT_HEAVY_THRESHOLD
     row_order: str | None = None
-    narrow_variant: int = 5
+    narrow_variant: int = 6
     balance: bool = True
+    autotune: bool = False
+    pad_lists: bool = True
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
         if self.row_order not in (None, "natural", "locality"):
             raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
-        if not 0 <= int(self.narrow_variant) < 6:
-            raise ValueError(f"narrow_variant must be in [0, 6), got {self.narrow_variant}")
+        if not 0 <= int(self.narrow_variant) < 7:
+            raise ValueError(f"narrow_variant must be in [0, 7), got {self.narrow_variant}")
+        if int(self.narrow_variant) == 6 and not self.pad_lists:
+            raise ValueError("narrow_variant 6 reads padded gather lists; it needs pad_lists=True")
 
     def locality(self, direction: Direction) -> bool:
         if self.row_order is None:
@@ -85,14 +92,15 @@ class B200Plan:
 
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
-        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance"}
+        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
         return cls(exact_order=bool(value.get("exact_order", False)),
                    heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)),
-                   row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 5)),
-                   balance=bool(value.get("balance", True)))
+                   row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 6)),
+                   balance=bool(value.get("balance", True)), autotune=bool(value.get("autotune", False)),
+                   pad_lists=bool(value.get("pad_lists", True)))
 
 
 @dataclass(frozen=True)
@@ -267,7 +275,8 @@ def _level_plans(artifact_index: int, scan: ArtifactScan, direction: Direction, 
         rows = int(scan.level_sizes[level])
         if rows == 0:
             continue
-        entries = up_entry_bound(scan, level) if direction == Direction.UP else down_entry_bound(scan, level, with_miss)
+        entries = (up_entry_bound(scan, level, plan.pad_lists) if direction == Direction.UP
+                   else down_entry_bound(scan, level, with_miss, plan.pad_lists))
         heavy = min(rows, entries // (int(plan.heavy_threshold) + 1))
         nbytes = blob_layout(rows, heavy, entries, True)[4]  # row map: locality order or heavy suffix
         out.append(LevelPlan(artifact_index, direction, level, pos, rows, entries, heavy, nbytes))

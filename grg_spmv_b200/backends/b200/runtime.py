@@ -165,6 +165,7 @@ class B200Runtime:
         self._ring = None
         self._artifacts = ()
         self._grgs = ()
+        self._variant = {}
         self._entered = False
         self._active_call = False
 
@@ -215,6 +216,10 @@ class B200Runtime:
                     self._ring = ring
                 self._artifacts = tuple(self._build_artifact(art) for art in lay.artifacts)
             self._grgs = tuple(self._bound_grg_cls(self, idx, art.state, art.path, lay.device) for idx, art in enumerate(self._artifacts))
+            for direction in (Direction.UP, Direction.DOWN):
+                plan = lay.pair.plan_for(direction)
+                if plan is not None and plan.autotune:
+                    self._variant[direction] = self._tune_direction(direction)
             self._entered = True
             return self
         except Exception:
@@ -274,14 +279,15 @@ class B200Runtime:
         off = np.asarray(st.level_offsets, dtype=np.int64)
         if up_on:
             plan = lay.pair.plan_up
-            built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance)}
+            built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance,
+                                                            plan.pad_lists)}
             levels[Direction.UP] = self._upload_levels(art.levels_up, built)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
             plan = lay.pair.plan_down
             built = {lv.level: lv for lv in build_down_levels(
                 off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
-                plan.locality(Direction.DOWN), plan.balance)}
+                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists)}
             levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
         del coo
         return _DeviceArtifact(
@@ -323,8 +329,48 @@ class B200Runtime:
             arr[i] = nat.Level(row_begin=lv.row_begin, num_rows=lv.num_rows, num_entries=lv.num_entries,
                                num_heavy=int(lv.heavy_rows.size), heavy_threshold=lv.heavy_threshold, ring_slot=slot,
                                blob=blob.data_ptr(), blob_bytes=nbytes, off_row_ptr=off_ptr, off_heavy=off_heavy,
-                               off_row_ids=off_ids, off_entries=off_entries)
+                               off_row_ids=off_ids, off_entries=off_entries, list_align=lv.list_align)
         return _DeviceLevels(array=arr, keepalive=keep)
+
+    # -- autotuning ------------------------------------------------------------------------------
+    TUNE_VARIANTS = (5, 6, 0, 1, 4)
+
+    def _tune_direction(self, direction: Direction) -> int:
+        """Fastest narrow-row kernel variant for ``direction`` on the first artifact at the
+        declared max k (the counterpart of ``TritonRuntime._tune_direction``,
+        ``pygrgl_spmv/backends/triton/backend.py:1062-1079``).  Each candidate runs once to
+        warm up and is then timed over three traversals with CUDA events."""
+        import torch
+
+        from grg_spmv_b200.grg import CudaMatmulSpec
+
+        art = self._artifacts[0]
+        st = art.state
+        k = int(self.layout.requirements.max_k_up if direction == Direction.UP else self.layout.requirements.max_k_down)
+        cols_in = st.num_samples if direction == Direction.UP else st.num_mutations
+        cols_out = st.num_mutations if direction == Direction.UP else st.num_samples
+        spec = CudaMatmulSpec(direction=direction, k=k, emit_all_nodes=False, by_individual=False, init_mode=InitMode.NONE,
+                              backend_init_mode=InitMode.NONE, use_miss=False, input_cols=cols_in, output_cols=cols_out,
+                              apply_endpoint_bias=False)
+        args = self._traverse_args(art, spec, self._io0[:cols_in, :k], self._io0[:cols_out, :k], None, None, None)
+        best, best_ms = None, None
+        with torch.cuda.device(self.device), torch.cuda.stream(self._caller_stream):
+            plan = self.layout.pair.plan_for(direction)
+            for variant in self.TUNE_VARIANTS:
+                if variant == 6 and not plan.pad_lists:
+                    continue
+                args.narrow_variant = variant
+                self._launch(args)
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record()
+                for _ in range(3):
+                    self._launch(args)
+                end.record()
+                end.synchronize()
+                ms = start.elapsed_time(end)
+                if best_ms is None or ms < best_ms:
+                    best, best_ms = variant, ms
+        return int(best)
 
     # -- calls ----------------------------------------------------------------------------------
     def _torch_caller_stream(self):
@@ -413,7 +459,7 @@ class B200Runtime:
             a.slot_bytes = ctypes.cast(self._slot_bytes, ctypes.POINTER(ctypes.c_int64))
             a.num_slots = len(self._slots)
         a.error_word = _ptr(self._error_word) if self._check_bounds else None
-        a.narrow_variant = int(plan.narrow_variant)
+        a.narrow_variant = int(self._variant.get(direction, plan.narrow_variant))
         return a
 
     def _capturing(self) -> bool:

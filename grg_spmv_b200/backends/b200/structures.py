@@ -59,6 +59,7 @@ class LevelGather:
     heavy_rows: np.ndarray  # int32 processing positions
     heavy_threshold: int
     row_ids: np.ndarray | None = None  # int32 level-local row of each position (None: identity)
+    list_align: int = 1  # 4: lists padded to multiples of 4 entries with null codes
 
     @property
     def num_entries(self) -> int:
@@ -98,7 +99,8 @@ def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.nd
 
 
 def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
-            group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True) -> LevelGather:
+            group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True,
+            pad: bool = False) -> LevelGather:
     """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr.
 
     With ``locality`` the rows are stored in the order of the id of their last state entry
@@ -144,9 +146,21 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
         gather = np.repeat(row_ptr[:-1][perm] - new_ptr[:-1], lengths) + np.arange(int(new_ptr[-1]), dtype=np.int64)
         entries = entries[gather]
         row_ptr, row_ids = new_ptr, perm.astype(np.int32)
+    counts = np.diff(row_ptr)
+    if pad:
+        # Every list starts at a multiple of 4 entries and holds a multiple of 4 (null padding).
+        padded = (counts + 3) // 4 * 4
+        new_ptr = np.zeros(num_rows + 1, dtype=np.int64)
+        np.cumsum(padded, out=new_ptr[1:])
+        out = np.full(int(new_ptr[-1]), np.uint32(nat.SRC_NULL << nat.SRC_SHIFT), dtype=np.uint32)
+        owner = np.repeat(np.arange(num_rows, dtype=np.int64), counts)
+        out[new_ptr[:-1][owner] + (np.arange(entries.size, dtype=np.int64) - row_ptr[:-1][owner])] = entries
+        entries, row_ptr = out, new_ptr
+        if row_ptr[-1] > np.iinfo(np.int32).max:
+            raise ValueError(f"level {level} has {int(row_ptr[-1])} padded entries, above the 2^31-1 per-level limit")
     heavy = np.arange(num_rows - num_heavy, num_rows, dtype=np.int32)
     return LevelGather(level, int(row_begin), int(num_rows), row_ptr.astype(np.int32), entries, heavy,
-                       int(heavy_threshold), row_ids)
+                       int(heavy_threshold), row_ids, 4 if pad else 1)
 
 
 def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
@@ -160,7 +174,7 @@ def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
 
 
 def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, locality: bool = False,
-                    balance: bool = True) -> list[LevelGather]:
+                    balance: bool = True, pad: bool = False) -> list[LevelGather]:
     """Gather lists for up levels 1..h-1 (level 0 is seeded from the input)."""
     off = np.asarray(level_offsets, dtype=np.int64)
     h = off.size - 1
@@ -177,7 +191,7 @@ def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, 
             src.append(np.full(r.size, s, dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
-        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance))
+        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad))
     return levels
 
 
@@ -191,7 +205,7 @@ def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[
 
 
 def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int,
-                      locality: bool = True, balance: bool = True) -> list[LevelGather]:
+                      locality: bool = True, balance: bool = True, pad: bool = False) -> list[LevelGather]:
     """Gather lists for down levels h-1..0 in execution order.
 
     ``sel_mut``/``sel_miss`` are (indptr, indices, num_mutations) triples; ``sel_miss`` may be
@@ -224,20 +238,21 @@ def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, h
             grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         levels.append(_finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
-                              cat(grp, np.int16), heavy_threshold, locality, balance))
+                              cat(grp, np.int16), heavy_threshold, locality, balance, pad))
     return levels
 
 
-def up_entry_bound(scan, level: int) -> int:
-    return int(sum(b.nnz for b in scan.blocks if b.dst_level == level))
+def up_entry_bound(scan, level: int, pad: bool = False) -> int:
+    total = sum(b.nnz for b in scan.blocks if b.dst_level == level)
+    return int(total + (3 * scan.level_sizes[level] if pad else 0))
 
 
-def down_entry_bound(scan, level: int, with_miss: bool) -> int:
+def down_entry_bound(scan, level: int, with_miss: bool, pad: bool = False) -> int:
     total = sum(b.nnz for b in scan.blocks if b.src_level == level)
     total += int(scan.selector_nnz_by_level[level, 0])
     if with_miss:
         total += int(scan.selector_nnz_by_level[level, 1])
-    return int(total)
+    return int(total + (3 * scan.level_sizes[level] if pad else 0))
 
 
 __all__ = [

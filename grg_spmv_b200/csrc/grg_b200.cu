@@ -137,6 +137,7 @@ struct LevelArgs {
     const int32_t* row_ids;
     int64_t num_heavy;
     int32_t heavy_threshold;
+    int32_t list_align;
     int32_t use_miss;
     void* state;
     int64_t ld_state;
@@ -206,7 +207,7 @@ __device__ __forceinline__ const T* entry_row(const LevelArgs& a, uint32_t code)
         }
         return static_cast<const T*>(a.x) + id * a.ld_x;
     }
-    if (!a.use_miss) return nullptr;
+    if (src != GRG_B200_SRC_MISS || !a.use_miss) return nullptr;  // null padding, or miss rows off
     if (a.err && id >= a.lim_miss) {
         report(a.err, kErrMissId);
         return nullptr;
@@ -239,9 +240,10 @@ __global__ void __launch_bounds__(kNarrowThreads, MIN_BLOCKS) level_narrow_kerne
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int rpw_log = 5 - a.log2g;  // positions per warp = 32 >> log2g
+    const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
     const int64_t pos0 = (static_cast<int64_t>(blockIdx.x) * kNarrowWarps + warp) << rpw_log;
-    if (pos0 >= a.num_rows) return;  // uniform across the warp
-    const int here = static_cast<int>(a.num_rows - pos0 < (int64_t(1) << rpw_log) ? a.num_rows - pos0 : (int64_t(1) << rpw_log));
+    if (pos0 >= narrow) return;  // uniform across the warp
+    const int here = static_cast<int>(narrow - pos0 < (int64_t(1) << rpw_log) ? narrow - pos0 : (int64_t(1) << rpw_log));
     // Lane l < here holds the list bounds of position pos0 + l (a full warp of single-lane
     // rows needs 33 offsets, so each lane loads both ends of its own position).
     int32_t lo = 0, hi = 0;
@@ -260,7 +262,7 @@ __global__ void __launch_bounds__(kNarrowThreads, MIN_BLOCKS) level_narrow_kerne
         for (int j = lane; j < span; j += 32) stage[warp][j] = __ldg(a.entries + span_begin + j);
     }
     __syncwarp();
-    if (my >= here || e1 - e0 > a.heavy_threshold) return;  // heavy rows: level_wide_kernel
+    if (my >= here) return;
     const int glane = lane & ((1 << a.log2g) - 1);
     const int64_t row = level_row(a, pos0 + my);
     T* state = static_cast<T*>(a.state);
@@ -392,6 +394,57 @@ __global__ void __launch_bounds__(kAsyncThreads) level_async_kernel(LevelArgs a)
             add_into(acc, seg);
             st_pack(state + row * a.ld_state + c, acc);
         }
+    }
+}
+
+// Narrow rows from padded lists (narrow_variant 6).  Same ownership as level_narrow_kernel; a
+// lane reads its row's codes four at a time with one aligned 16-byte load and loads the next
+// four while the current four rows are fetched, so each round waits on one memory latency.
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kNarrowThreads, 6) level_vec_kernel(LevelArgs a) {
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
+    const int64_t pos = ((static_cast<int64_t>(blockIdx.x) * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    if (pos >= narrow) return;  // no warp-wide operations below
+    const int32_t e0 = __ldg(a.row_ptr + pos);
+    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int64_t row = level_row(a, pos);
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(glane) * V; c < a.k; c += step) {
+        Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+        Pack<T, V> seg = zero_pack<T, V>();
+        const int32_t q1 = e1 >> 2;
+        int32_t q = e0 >> 2;
+        uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
+        for (; q < q1; ++q) {
+            const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+            const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+            Pack<T, V> val[4];
+            bool valid[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const T* src = entry_row<T>(a, code[u]);
+                valid[u] = src != nullptr;
+                val[u] = valid[u] ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (code[u] & GRG_B200_SEG_START) {
+                    add_into(acc, seg);
+                    seg = zero_pack<T, V>();
+                }
+                if (valid[u]) add_into(seg, val[u]);
+            }
+            cur = nxt;
+        }
+        add_into(acc, seg);
+        st_pack(state + row * a.ld_state + c, acc);
     }
 }
 
@@ -695,7 +748,17 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
 template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    if (narrow > 0 && variant == 4) {
+    if (narrow > 0 && variant == 6) {
+        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
+        switch (init_mode) {
+            case 0: level_vec_kernel<T, V, 0><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 1: level_vec_kernel<T, V, 1><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 2: level_vec_kernel<T, V, 2><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            default: level_vec_kernel<T, V, 3><<<grid, kNarrowThreads, 0, s>>>(la); break;
+        }
+        GRG_LAUNCH_CHECK("level_vec_kernel");
+    } else if (narrow > 0 && variant == 4) {
         const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
         const dim3 grid(static_cast<unsigned>((warps + kAsyncWarps - 1) / kAsyncWarps));
         switch (init_mode) {
@@ -771,6 +834,11 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     la.entries = reinterpret_cast<const uint32_t*>(base + L->off_entries);
     la.heavy_rows = reinterpret_cast<const int32_t*>(base + L->off_heavy);
     la.row_ids = L->off_row_ids >= 0 ? reinterpret_cast<const int32_t*>(base + L->off_row_ids) : nullptr;
+    if (L->list_align != 1 && L->list_align != 4) return fail(GRG_B200_ERR_INVALID, "list_align must be 1 or 4, got %d", L->list_align);
+    if (a->narrow_variant == 6 && L->list_align != 4)
+        return fail(GRG_B200_ERR_INVALID, "narrow_variant 6 needs padded gather lists (list_align 4)");
+    if (L->list_align == 4 && (L->off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
+    la.list_align = L->list_align;
     la.num_heavy = L->num_heavy;
     la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
     const bool exact = a->exact_order != 0;

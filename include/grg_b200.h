@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 3
+#define GRG_B200_ABI_VERSION 4
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -85,6 +85,7 @@ typedef enum grg_b200_bias {
 #define GRG_B200_SRC_STATE 0u /* id = state row */
 #define GRG_B200_SRC_INPUT 1u /* id = input row (down: mutation) */
 #define GRG_B200_SRC_MISS 2u  /* id = miss row (down: mutation), skipped unless use_miss */
+#define GRG_B200_SRC_NULL 3u  /* padding entry: skipped, never flagged as a segment start */
 #define GRG_B200_ID_MASK 0x1FFFFFFFu
 #define GRG_B200_MAX_ID 0x1FFFFFFFu
 
@@ -98,6 +99,9 @@ typedef enum grg_b200_bias {
  *   int32  heavy_rows[num_heavy]     the heavy positions (num_rows - num_heavy, ...)
  *   int32  row_ids[num_rows]         optional processing position -> level-local row
  *   uint32 entries[num_entries]
+ * list_align = 4: every position's list starts at a multiple of 4 entries and holds a
+ * multiple of 4 entries (null-padded), so kernels may read 4 codes with one 16-byte load
+ * (narrow variant 6 requires it); list_align = 1: no padding.
  * ring_slot < 0: blob is device memory.  ring_slot >= 0: blob is pinned host memory that
  * grg_b200_traverse copies into ring slot `ring_slot` before the level runs.
  */
@@ -114,6 +118,8 @@ typedef struct grg_b200_level {
     int64_t off_heavy;
     int64_t off_row_ids; /* -1: identity order */
     int64_t off_entries;
+    int32_t list_align;  /* 1 or 4 */
+    int32_t reserved;
 } grg_b200_level;
 
 typedef struct grg_b200_ring grg_b200_ring; /* opaque: copy stream + per-slot events */
@@ -167,10 +173,12 @@ typedef struct grg_b200_traverse_args {
                                            round from a shared-memory staged list; 3: 16 rows per
                                            round, staged; 4: cp.async gathers into shared memory,
                                            then in-order sums; 5: as 0 with at most 32 registers
-                                           per thread (8 CTAs per SM). */
+                                           per thread (8 CTAs per SM); 6: padded lists (list_align
+                                           4) read 4 codes per 16-byte load, next 4 prefetched
+                                           while the current 4 rows load. */
 } grg_b200_traverse_args;
 
-#define GRG_B200_NARROW_VARIANTS 6
+#define GRG_B200_NARROW_VARIANTS 7
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

@@ -27,7 +27,7 @@ def _row_sum(codes, state, x, miss, acc):
             seg = seg + state[i]
         elif src == nat.SRC_INPUT:
             seg = seg + x[i]
-        elif miss is not None:
+        elif src == nat.SRC_MISS and miss is not None:
             seg = seg + miss[i]
     return acc + seg
 
@@ -59,14 +59,14 @@ def model_matmul(path, x, direction, dtype=np.float64, *, init=None, miss=None, 
             if r < st.num_samples:
                 v = v + xi[s2i[r] if by_individual else r]
             state[r] = v
-        for lv in build_up_levels(off, coo, 1 << 30, locality=True):
+        for lv in build_up_levels(off, coo, 1 << 30, locality=True, pad=True):
             for r, codes in lv.row_lists():
                 state[lv.row_begin + r] = _row_sum(codes, state, xi, None, init_row(lv.row_begin + r))
     else:
         sel_mut = (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations)
         sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations)
         mi = None if miss is None else np.ascontiguousarray(miss.T.astype(dt))
-        for lv in build_down_levels(off, coo, sel_mut, sel_miss, 1 << 30, locality=True):
+        for lv in build_down_levels(off, coo, sel_mut, sel_miss, 1 << 30, locality=True, pad=True):
             for r, codes in lv.row_lists():
                 state[lv.row_begin + r] = _row_sum(codes, state, xi, mi, init_row(lv.row_begin + r))
     if emit_all_nodes:

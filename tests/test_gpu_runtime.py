@@ -102,7 +102,7 @@ def test_up_output_aliases_down_input():
 
 
 @pytest.mark.parametrize("k", [1, 2, 3, 5, 8, 16, 33])
-@pytest.mark.parametrize("variant", [0, 4])
+@pytest.mark.parametrize("variant", [0, 4, 5, 6])
 def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     """Integer-valued inputs are exact; real-valued inputs agree to 1e-12 (default heavy-row
     reduction) — every mode of the hot path on a 60k-node graph with random node ids."""
@@ -331,3 +331,18 @@ def test_foreign_stream_ordering(synth_artifact):
             out = op.output.clone()
         stream.synchronize()
         np.testing.assert_allclose(out.cpu().numpy(), oracle.matmul(x, "up"), rtol=1e-12, atol=1e-9)
+
+
+def test_autotune_picks_a_known_variant_and_stays_exact(synth_artifact):
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
+
+    oracle = OracleGRG(synth_artifact)
+    pair = B200PlanPair(plan_up=B200Plan(autotune=True), plan_down=B200Plan(autotune=True))
+    rng = np.random.default_rng(13)
+    with _runtime(_layout([synth_artifact], requirements=_req(k=4), pair=pair)) as runtime:
+        assert set(runtime._variant) == {"up", "down"}
+        assert all(v in B200Runtime.TUNE_VARIANTS for v in runtime._variant.values())
+        (grg,) = runtime.grgs
+        for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
+            x = _pm1(rng, (4, cols))
+            np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))

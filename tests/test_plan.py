@@ -122,9 +122,9 @@ def test_planned_bytes_bound_the_built_level_blobs(name, heavy):
     layout = _plan((name,), pair=pair)
     st = load_grg_spmv_header(artifact_path(name), np.float64)
     coo = load_blocks(iter_artifact_blocks(artifact_path(name)))
-    up = {lv.level: lv for lv in build_up_levels(st.level_offsets, coo, heavy, False)}
+    up = {lv.level: lv for lv in build_up_levels(st.level_offsets, coo, heavy, False, True, True)}
     down = {lv.level: lv for lv in build_down_levels(st.level_offsets, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations),
-                                                     (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations), heavy, True)}
+                                                     (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations), heavy, True, True, True)}
     for lp in layout.artifacts[0].levels_up:
         assert up[lp.level].layout()[4] <= lp.nbytes
     for lp in layout.artifacts[0].levels_down:
