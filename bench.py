@@ -52,7 +52,7 @@ def parse_args():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["b200", "reference"], default="b200")
     p.add_argument("--k", type=int, default=8)
-    p.add_argument("--workload", choices=["config2", "small"], default="config2")
+    p.add_argument("--workload", choices=["config2", "medium", "small"], default="config2")
     p.add_argument("--exact-order", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -62,7 +62,8 @@ def parse_args():
     p.add_argument("--variant", type=int, default=None, help="narrow-row kernel variant")
     p.add_argument("--no-graphs", action="store_true", help="launch kernels per level instead of replaying a CUDA graph")
     p.add_argument("--no-balance", action="store_true", help="do not group narrow rows by length")
-    p.add_argument("--autotune", action="store_true", help="pick the narrow-kernel variant per direction at runtime entry")
+    p.add_argument("--autotune", action="store_true", help="pick the narrow and heavy kernels per direction at runtime entry")
+    p.add_argument("--heavy-variant", type=int, default=None, help="heavy-row kernel: 0 CTA per row, 1 warp per row")
     p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
     p.add_argument("--row-order-down", choices=["natural", "locality"], default=None)
     return p.parse_args()
@@ -73,6 +74,9 @@ def workload_spec(name: str, seed: int):
 
     if name == "config2":
         return dataclasses.replace(CONFIG2, seed=seed)
+    if name == "medium":  # profiling case: the same generator at 30% scale, working set still above L2
+        return SynthSpec(num_samples=30_000, num_levels=40, num_nodes=1_500_000, num_mutations=300_000, children=(2, 22),
+                         miss_fraction=0.01, seed=seed)
     return SynthSpec(num_samples=20_000, num_levels=20, num_nodes=600_000, num_mutations=100_000, children=(2, 28),
                      miss_fraction=0.01, seed=seed)
 
@@ -203,6 +207,8 @@ def run_b200(args) -> None:
         extra["balance"] = False
     if args.autotune:
         extra["autotune"] = True
+    if args.heavy_variant is not None:
+        extra["heavy_variant"] = args.heavy_variant
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
                         plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
     stream = torch.cuda.Stream(device=device)
@@ -372,7 +378,8 @@ def run_b200(args) -> None:
         rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-300))
         max_rel = max(rel(got_up, ref_up), rel(got_down, ref_down))
 
-    tuned = {d.value: v for d, v in runtime._variant.items()}
+    tuned = {d.value: [v, runtime._heavy_variant.get(d)] for d, v in runtime._variant.items()}
+    heavy_used = {"up": int(up._args.heavy_variant), "down": int(down._args.heavy_variant)}
     runtime.__exit__(None, None, None)
     if rank == 0:
         line = {
@@ -394,12 +401,12 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": pair.plan_down.narrow_variant,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "autotuned_variants": tuned,
+                       "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
                        "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "level gather (level_narrow_kernel + level_wide_kernel)",
+                         "traffic": None, "kernel": "level gathers (narrow-row kernel of the plan + heavy-row kernel)",
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
                          "level_ms_per_step": level_total_ms, "level_bytes_per_step": lv_bytes},
             "cpu_baseline": cpu,

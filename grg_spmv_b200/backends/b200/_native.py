@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 4
+ABI_VERSION = 6
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -27,11 +27,28 @@ NVCC_FLAGS = (
 
 # Status codes, enums and entry coding (grg_b200.h).
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED = 0, 1, 2, 3
-F64, F32 = 0, 1
+F64, F32, MIXED = 0, 1, 2
 UP, DOWN = 0, 1
 INIT_NONE, INIT_VECTOR, INIT_XTX, INIT_MATRIX = 0, 1, 2, 3
 BIAS_NONE, BIAS_VECTOR, BIAS_XTX = 0, 1, 2
 SEG_START = 0x80000000
+
+
+def mix_plane(nbytes: int) -> int:
+    """GRG_B200_MIX_PLANE: a plane's bytes rounded up to 16."""
+    return (int(nbytes) + 15) // 16 * 16
+
+
+def mix_bytes(rows: int, ld: int) -> int:
+    """GRG_B200_MIX_BYTES: one mixed buffer (float hi plane, then int16 lo plane)."""
+    return mix_plane(int(rows) * int(ld) * 4) + mix_plane(int(rows) * int(ld) * 2)
+
+
+def mix_ld(k: int) -> int:
+    """Leading dimension of mixed storage for k columns (a multiple of 4)."""
+    return (int(k) + 3) // 4 * 4
+
+
 SRC_SHIFT = 29
 SRC_STATE, SRC_INPUT, SRC_MISS, SRC_NULL = 0, 1, 2, 3
 ID_MASK = 0x1FFFFFFF
@@ -104,6 +121,9 @@ class TraverseArgs(ctypes.Structure):
         ("num_slots", ctypes.c_int32),
         ("error_word", ctypes.c_void_p),
         ("narrow_variant", ctypes.c_int32),
+        ("heavy_variant", ctypes.c_int32),
+        ("mix_scratch", ctypes.c_void_p),
+        ("mix_scratch_bytes", ctypes.c_int64),
     ]
 
 

@@ -56,15 +56,19 @@ class B200Plan:
     ``exact_order``: heavy rows are also summed in list order, which makes every result
     bit-identical to the reference's ReferenceRuntime (default: heavy rows are split over a
     CTA and tree-reduced, deterministic and exact for integer-valued data).
-    ``heavy_threshold``: rows with more entries than this are processed one CTA per row.
+    ``heavy_threshold``: rows with more entries than this go to the heavy-row kernel.
     ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
     processed together); None picks the direction's default (up natural, down locality).
     ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``).
     ``balance``: group narrow rows by length (power-of-two buckets) so a warp's rows finish
     together.
-    ``autotune``: time the narrow-kernel variants when the runtime is entered and use the
-    fastest for this direction (instead of ``narrow_variant``).
+    ``autotune``: time the narrow-kernel variants, then the heavy-row kernels, when the runtime
+    is entered and use the fastest for this direction (instead of ``narrow_variant`` and
+    ``heavy_variant``).
     ``pad_lists``: pad every gather list to a multiple of 4 entries (needed by variant 6).
+    ``heavy_variant``: heavy rows one warp each (1) or one CTA each (0); None picks per call
+    (warp for k <= 16, where a warp still splits a list over >= 4 lane groups; CTA above).
+    Exact order always uses CTAs.
     """
 
     exact_order: bool = False
@@ -74,6 +78,7 @@ class B200Plan:
     balance: bool = True
     autotune: bool = False
     pad_lists: bool = True
+    heavy_variant: int | None = None
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -84,6 +89,8 @@ class B200Plan:
             raise ValueError(f"narrow_variant must be in [0, 7), got {self.narrow_variant}")
         if int(self.narrow_variant) == 6 and not self.pad_lists:
             raise ValueError("narrow_variant 6 reads padded gather lists; it needs pad_lists=True")
+        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1):
+            raise ValueError(f"heavy_variant must be 0 or 1, got {self.heavy_variant}")
 
     def locality(self, direction: Direction) -> bool:
         if self.row_order is None:
@@ -92,7 +99,8 @@ class B200Plan:
 
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
-        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists"}
+        allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
+                   "heavy_variant"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -100,7 +108,7 @@ class B200Plan:
                    heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)),
                    row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 6)),
                    balance=bool(value.get("balance", True)), autotune=bool(value.get("autotune", False)),
-                   pad_lists=bool(value.get("pad_lists", True)))
+                   pad_lists=bool(value.get("pad_lists", True)), heavy_variant=value.get("heavy_variant"))
 
 
 @dataclass(frozen=True)
@@ -148,6 +156,8 @@ class B200Layout:
     artifacts: tuple[ArtifactLayout, ...]
     pair: B200PlanPair
     dtype: np.dtype
+    precision: str
+    mix_scratch_bytes: int
     requirements: object
     device: int
     stream_ptr: int
@@ -326,11 +336,21 @@ def plan_b200_layout(
     device,
     stream,
     pair: B200PlanPair | None = None,
+    precision: str = "plain",
 ) -> B200Layout:
+    """Plan device memory for ``artifacts`` (the counterpart of ``plan_triton_layout``,
+    ``pygrgl_spmv/backends/triton/backend.py:343-371``).
+
+    ``precision="plain"`` computes and stores in ``dtype``.  ``precision="mixed"`` (``dtype``
+    must be float64: inputs and outputs stay FP64) keeps the node state in 6 bytes per value,
+    an FP32 value plus a 16-bit correction (relative rounding <= 2^-40 per node, integers below
+    2^40 exact), with FP64 accumulation; it needs padded lists and the default (not
+    exact-order) heavy-row mode."""
     dtype = np.dtype(dtype)
     if dtype not in (np.dtype(np.float32), np.dtype(np.float64)):
         raise ValueError(f"B200 runtime supports only float32/float64, got {dtype}")
     pair = B200PlanPair() if pair is None else pair
+    _check_precision(precision, dtype, pair)
     requested_ring = int(ring_buffer_size)
     requested_budget = int(vram_budget_bytes)
     if requested_ring < 0:
@@ -348,12 +368,39 @@ def plan_b200_layout(
     return plan_layout_from_scans(
         scans=tuple(scan_grg_spmv(p) for p in paths), paths=paths, dtype=dtype, requirements=requirements,
         requested_budget=requested_budget, requested_ring=requested_ring, allow_residency=bool(allow_residency),
-        device_id=device_id, stream_ptr=stream_ptr, stream_owner=stream_owner, pair=pair)
+        device_id=device_id, stream_ptr=stream_ptr, stream_owner=stream_owner, pair=pair, precision=precision)
+
+
+PRECISIONS = ("plain", "mixed")
+
+
+def _check_precision(precision: str, dtype, pair: B200PlanPair) -> None:
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {PRECISIONS}, got {precision!r}")
+    if precision != "mixed":
+        return
+    if np.dtype(dtype) != np.dtype(np.float64):
+        raise ValueError("precision='mixed' keeps FP64 inputs and outputs; pass dtype=np.float64")
+    for plan in (pair.plan_up, pair.plan_down):
+        if plan is not None and (plan.exact_order or not plan.pad_lists):
+            raise ValueError("precision='mixed' needs pad_lists=True and exact_order=False")
+
+
+def mixed_state_bytes(num_nodes: int, max_k: int) -> int:
+    """Node state of mixed precision: float hi plane + int16 lo plane, ld = k rounded up to 4."""
+    ld = (int(max_k) + 3) // 4 * 4
+    return _plane(num_nodes * ld * 4) + _plane(num_nodes * ld * 2)
+
+
+def _plane(nbytes: int) -> int:
+    return (int(nbytes) + 15) // 16 * 16
 
 
 def plan_layout_from_scans(*, scans, paths, dtype, requirements, requested_budget: int, requested_ring: int,
-                           allow_residency: bool, device_id: int, stream_ptr: int, stream_owner, pair: B200PlanPair) -> B200Layout:
+                           allow_residency: bool, device_id: int, stream_ptr: int, stream_owner, pair: B200PlanPair,
+                           precision: str = "plain") -> B200Layout:
     """The device-independent part of the planner (exercised by the CPU tests)."""
+    _check_precision(precision, dtype, pair)
     itemsize = int(np.dtype(dtype).itemsize)
     max_S = max(s.num_samples for s in scans)
     max_M = max(s.num_mutations for s in scans)
@@ -388,11 +435,16 @@ def plan_layout_from_scans(*, scans, paths, dtype, requirements, requested_budge
         artifacts.append(ArtifactLayout(path=Path(path), scan=scan, levels_up=lu, levels_down=ld))
 
     state_bytes = max_N * max_k * itemsize
+    mix_scratch = 0
+    if precision == "mixed":
+        state_bytes = mixed_state_bytes(max_N, max_k)
+        if down_on:  # encoded down input (and miss) rows
+            mix_scratch = mixed_state_bytes(max_M, max_k) * (2 if down_miss else 1)
     io0_rows = max(max_S, max_M)
     io1_rows = side_io_rows(pair, requirements, max_num_mutations=max_M, max_num_nodes=max_N)
     aux_rows = max_N  # all-node output
     dense_arena = (io0_rows + io1_rows + aux_rows) * max_k * itemsize
-    scratch = 256  # device error word
+    scratch = 256 + mix_scratch  # device error word (+ mixed-precision encoded down inputs)
     fixed = selectors + metadata + xtx + state_bytes + dense_arena + scratch
     resident_full = sum(lp.nbytes for lp in all_levels)
     required_full = fixed + resident_full
@@ -458,6 +510,8 @@ def plan_layout_from_scans(*, scans, paths, dtype, requirements, requested_budge
         artifacts=tuple(artifacts),
         pair=pair,
         dtype=np.dtype(dtype),
+        precision=precision,
+        mix_scratch_bytes=int(mix_scratch),
         requirements=requirements,
         device=device_id,
         stream_ptr=stream_ptr,

@@ -155,6 +155,7 @@ class B200Runtime:
         self._caller_stream = None
         self.stream = None
         self._state = None
+        self._mix_scratch = None
         self._io0 = None
         self._io1 = None
         self._aux = None
@@ -166,6 +167,7 @@ class B200Runtime:
         self._artifacts = ()
         self._grgs = ()
         self._variant = {}
+        self._heavy_variant = {}
         self._entered = False
         self._active_call = False
 
@@ -199,7 +201,13 @@ class B200Runtime:
             with torch.cuda.device(self.device):
                 self._caller_stream = torch.cuda.get_stream_from_external(self.stream_ptr, device=self.device)
                 self.stream = self._caller_stream
-                self._state = torch.zeros(lay.max_num_nodes * max_k, device=self.device, dtype=tdt)
+                if lay.precision == "mixed":  # float hi plane + int16 lo plane (grg_b200.h GRG_B200_MIXED)
+                    self._state = torch.zeros(nat.mix_bytes(lay.max_num_nodes, nat.mix_ld(max_k)), device=self.device,
+                                              dtype=torch.uint8)
+                    if lay.mix_scratch_bytes:
+                        self._mix_scratch = torch.zeros(lay.mix_scratch_bytes, device=self.device, dtype=torch.uint8)
+                else:
+                    self._state = torch.zeros(lay.max_num_nodes * max_k, device=self.device, dtype=tdt)
                 self._io0 = torch.zeros((max(lay.max_num_samples, lay.max_num_mutations), max_k), device=self.device, dtype=tdt)
                 io1_rows = side_io_rows(lay.pair, lay.requirements, max_num_mutations=lay.max_num_mutations,
                                         max_num_nodes=lay.max_num_nodes)
@@ -218,8 +226,8 @@ class B200Runtime:
             self._grgs = tuple(self._bound_grg_cls(self, idx, art.state, art.path, lay.device) for idx, art in enumerate(self._artifacts))
             for direction in (Direction.UP, Direction.DOWN):
                 plan = lay.pair.plan_for(direction)
-                if plan is not None and plan.autotune:
-                    self._variant[direction] = self._tune_direction(direction)
+                if plan is not None and plan.autotune and lay.precision == "plain":
+                    self._variant[direction], self._heavy_variant[direction] = self._tune_direction(direction)
             self._entered = True
             return self
         except Exception:
@@ -335,11 +343,12 @@ class B200Runtime:
     # -- autotuning ------------------------------------------------------------------------------
     TUNE_VARIANTS = (5, 6, 0, 1, 4)
 
-    def _tune_direction(self, direction: Direction) -> int:
-        """Fastest narrow-row kernel variant for ``direction`` on the first artifact at the
-        declared max k (the counterpart of ``TritonRuntime._tune_direction``,
-        ``pygrgl_spmv/backends/triton/backend.py:1062-1079``).  Each candidate runs once to
-        warm up and is then timed over three traversals with CUDA events."""
+    def _tune_direction(self, direction: Direction) -> tuple[int, int]:
+        """Fastest (narrow variant, heavy variant) for ``direction`` on the first artifact at
+        the declared max k (the counterpart of ``TritonRuntime._tune_direction``,
+        ``pygrgl_spmv/backends/triton/backend.py:1062-1079``): narrow variants first, then the
+        two heavy-row kernels with the chosen narrow variant.  Each candidate runs once to warm
+        up and is then timed over three traversals with CUDA events."""
         import torch
 
         from grg_spmv_b200.grg import CudaMatmulSpec
@@ -353,24 +362,31 @@ class B200Runtime:
                               backend_init_mode=InitMode.NONE, use_miss=False, input_cols=cols_in, output_cols=cols_out,
                               apply_endpoint_bias=False)
         args = self._traverse_args(art, spec, self._io0[:cols_in, :k], self._io0[:cols_out, :k], None, None, None)
-        best, best_ms = None, None
+        plan = self.layout.pair.plan_for(direction)
+
+        def timed() -> float:
+            self._launch(args)
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record()
+            for _ in range(3):
+                self._launch(args)
+            end.record()
+            end.synchronize()
+            return start.elapsed_time(end)
+
         with torch.cuda.device(self.device), torch.cuda.stream(self._caller_stream):
-            plan = self.layout.pair.plan_for(direction)
+            narrow_ms = {}
             for variant in self.TUNE_VARIANTS:
                 if variant == 6 and not plan.pad_lists:
                     continue
                 args.narrow_variant = variant
-                self._launch(args)
-                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                start.record()
-                for _ in range(3):
-                    self._launch(args)
-                end.record()
-                end.synchronize()
-                ms = start.elapsed_time(end)
-                if best_ms is None or ms < best_ms:
-                    best, best_ms = variant, ms
-        return int(best)
+                narrow_ms[variant] = timed()
+            args.narrow_variant = min(narrow_ms, key=narrow_ms.get)
+            heavy_ms = {}
+            for heavy in (0, 1):
+                args.heavy_variant = heavy
+                heavy_ms[heavy] = timed()
+        return int(args.narrow_variant), int(min(heavy_ms, key=heavy_ms.get))
 
     # -- calls ----------------------------------------------------------------------------------
     def _torch_caller_stream(self):
@@ -395,7 +411,8 @@ class B200Runtime:
             raise ValueError("DOWN plan is not configured")
         return B200PreparedMatmul(self, self._artifacts[int(grg._artifact_index)], spec)
 
-    def _traverse_args(self, art: _DeviceArtifact, spec, input_view, output_view, miss_view, init_vector, init_matrix):
+    def _traverse_args(self, art: _DeviceArtifact, spec, input_view, output_view, miss_view, init_vector, init_matrix, *,
+                       state=None, mixed: bool | None = None, mix_scratch=None):
         st = art.state
         k = int(spec.k)
         direction = Direction(spec.direction)
@@ -413,7 +430,10 @@ class B200Runtime:
         if backend_init == InitMode.XTX and art.xtx_node is None:
             raise ValueError("init_mode=xtx requires GRG coalescence counts")
         a = nat.TraverseArgs()
-        a.dtype = nat.F64 if self.layout.dtype == np.float64 else nat.F32
+        mixed = self.layout.precision == "mixed" if mixed is None else bool(mixed)
+        state = self._state if state is None else state
+        mix_scratch = self._mix_scratch if mix_scratch is None else mix_scratch
+        a.dtype = nat.MIXED if mixed else (nat.F64 if self.layout.dtype == np.float64 else nat.F32)
         a.direction = nat.UP if direction == Direction.UP else nat.DOWN
         a.init_mode = _INIT_CODE[backend_init]
         a.bias_mode = bias_mode
@@ -426,8 +446,11 @@ class B200Runtime:
         a.num_samples = st.num_samples
         a.num_mutations = st.num_mutations
         a.num_individuals = st.num_individuals
-        a.state = _ptr(self._state)
-        a.ld_state = k
+        a.state = _ptr(state)
+        a.ld_state = nat.mix_ld(k) if mixed else k
+        if mixed and mix_scratch is not None:
+            a.mix_scratch = _ptr(mix_scratch)
+            a.mix_scratch_bytes = int(mix_scratch.numel())
         a.input = _ptr(input_view)
         a.ld_input = int(input_view.stride(0))
         a.output = _ptr(output_view)
@@ -460,6 +483,8 @@ class B200Runtime:
             a.num_slots = len(self._slots)
         a.error_word = _ptr(self._error_word) if self._check_bounds else None
         a.narrow_variant = int(self._variant.get(direction, plan.narrow_variant))
+        heavy = self._heavy_variant.get(direction, plan.heavy_variant)
+        a.heavy_variant = int(heavy) if heavy is not None else (1 if k <= 16 else 0)
         return a
 
     def _capturing(self) -> bool:
@@ -498,6 +523,15 @@ class B200Runtime:
                 return
             status = self._lib.grg_b200_traverse(ctypes.byref(args), ctypes.c_void_p(self.stream_ptr))
         nat.check(self._lib, status, "grg_b200_traverse")
+
+    def prepare_batch(self, items, *, precision: str | None = None, tile_k: int | None = None, autotune: bool = False):
+        """Several (grg, direction, k) matmuls run together as one CUDA graph; see
+        ``grg_spmv_b200.backends.b200.batch.B200BatchedMatmul``."""
+        from .batch import B200BatchedMatmul
+
+        if not self._entered:
+            raise RuntimeError("B200Runtime must be entered before preparing a batch")
+        return B200BatchedMatmul(self, items, precision=precision, tile_k=tile_k, autotune=autotune)
 
     def device_error(self) -> int:
         """Synchronise the caller stream and return the first failed device bounds check (0 = none)."""

@@ -156,6 +156,10 @@ struct LevelArgs {
     int64_t lim_state;
     int64_t lim_x;
     int64_t lim_miss;
+    // mixed storage only: the 16-bit planes of state, x and miss (x/miss hold encoded copies)
+    void* state_lo;
+    const void* x_lo;
+    const void* miss_lo;
 };
 
 enum DeviceError : int32_t {
@@ -448,6 +452,372 @@ __global__ void __launch_bounds__(kNarrowThreads, 6) level_vec_kernel(LevelArgs 
     }
 }
 
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> shfl_xor_pack(const Pack<T, V>& x, int off) {
+    Pack<T, V> r;
+#pragma unroll
+    for (int i = 0; i < V; ++i) r.v[i] = __shfl_xor_sync(kFullMask, x.v[i], off);
+    return r;
+}
+
+constexpr int kWarpRowThreads = 256;
+
+// Heavy rows, one warp each (heavy_variant 1, default mode only).  Lane group g of 32/G
+// groups takes every (32/G)-th 4-entry quad of the row's list (or every (32/G)-th entry for
+// unpadded lists) and fetches its rows independently; the groups' partial sums are combined
+// by an xor-shuffle butterfly in a fixed order, so the result is deterministic (and exact for
+// integer data), and group 0 adds the init value and stores the row.  Compared with a CTA per
+// row this keeps eight heavy rows per CTA and needs no shared memory or block barriers.
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a) {
+    const int64_t w = static_cast<int64_t>(blockIdx.x) * (kWarpRowThreads / 32) + (threadIdx.x >> 5);
+    if (w >= a.num_heavy) return;  // warp-uniform
+    const int lane32 = threadIdx.x & 31;
+    const int64_t pos = __ldg(a.heavy_rows + w);
+    const int32_t e0 = __ldg(a.row_ptr + pos);
+    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
+    const int64_t row = level_row(a, pos);
+    const int g_lanes = 1 << a.log2g;
+    const int groups = 32 >> a.log2g;
+    const int glane = lane32 & (g_lanes - 1);
+    const int grp = lane32 >> a.log2g;
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t base = 0; base < a.k; base += step) {  // uniform trip count across the warp
+        const int64_t c = base + static_cast<int64_t>(glane) * V;
+        const bool active = c < a.k;
+        Pack<T, V> part = zero_pack<T, V>();
+        if (active) {
+            if (a.list_align == 4) {
+                const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+                for (int32_t q = (e0 >> 2) + grp; q < (e1 >> 2); q += groups) {
+                    const uint4 cq = __ldg(codes4 + q);
+                    const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
+                    Pack<T, V> val[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const T* src = entry_row<T>(a, code[u]);
+                        val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) add_into(part, val[u]);
+                }
+            } else {
+                constexpr int UW = 4;
+                for (int32_t j = e0 + grp; j < e1; j += groups * UW) {
+                    Pack<T, V> val[UW];
+#pragma unroll
+                    for (int u = 0; u < UW; ++u) {
+                        const int32_t jj = j + u * groups;
+                        const T* src = jj < e1 ? entry_row<T>(a, __ldg(a.entries + jj)) : nullptr;
+                        val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                    }
+#pragma unroll
+                    for (int u = 0; u < UW; ++u) add_into(part, val[u]);
+                }
+            }
+        }
+        for (int off = 16; off >= g_lanes; off >>= 1) {
+            const Pack<T, V> other = shfl_xor_pack(part, off);
+            add_into(part, other);
+        }
+        if (grp == 0 && active) {
+            Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+            add_into(acc, part);
+            st_pack(state + row * a.ld_state + c, acc);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Mixed storage (dtype GRG_B200_MIXED)
+//
+// A value v is stored in 6 bytes as hi = v rounded to FP32 plus a 16-bit signed correction
+// lo, so that v ~= hi + lo * 2^(e(hi) - 39), where e(hi) is hi's unbiased exponent (FP32
+// subnormals use the smallest normal exponent).  hi carries 24 significant bits and lo 16
+// more, so a stored value is within 2^-40 of v relative to |hi| and integers below 2^40 are
+// exact.  Decoding is exact in FP64 (24 + 16 bits fit in 53), every sum is accumulated in
+// FP64 registers and rounded back to 6 bytes once per node.  A buffer of R rows and ld
+// columns (ld % 4 == 0) is two planes: float hi[R * ld] followed by int16 lo[R * ld].
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t mx_exp_field(float hi) {
+    const uint32_t e = (__float_as_uint(hi) >> 23) & 0xffu;
+    return e == 0u ? 1u : e;
+}
+
+// 2^(e - 39) for the biased exponent field E = e + 127: 2^(E - 166) as a double.
+__device__ __forceinline__ double mx_unit(float hi) {
+    return __longlong_as_double(static_cast<long long>(mx_exp_field(hi) + (1023u - 166u)) << 52);
+}
+
+__device__ __forceinline__ double mx_inv_unit(float hi) {
+    return __longlong_as_double(static_cast<long long>((1023u + 166u) - mx_exp_field(hi)) << 52);
+}
+
+__device__ __forceinline__ double mx_decode(float hi, short lo) {
+    return static_cast<double>(hi) + static_cast<double>(lo) * mx_unit(hi);
+}
+
+__device__ __forceinline__ void mx_encode(double v, float& hi, short& lo) {
+    hi = __double2float_rn(v);
+    if (!isfinite(hi)) {
+        lo = 0;
+        return;
+    }
+    const double r = v - static_cast<double>(hi);  // exact
+    int q = __double2int_rn(r * mx_inv_unit(hi));    // |q| <= 2^15
+    q = q > 32767 ? 32767 : (q < -32768 ? -32768 : q);
+    lo = static_cast<short>(q);
+}
+
+struct Quad {
+    double v[4];
+};
+
+__device__ __forceinline__ Quad zero_quad() { return Quad{{0.0, 0.0, 0.0, 0.0}}; }
+
+__device__ __forceinline__ void add_quad(Quad& a, const Quad& b) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) a.v[i] = a.v[i] + b.v[i];
+}
+
+// Four encoded columns [c, c + 4) as loaded (16-byte hi load + 8-byte lo load).
+struct RawQuad {
+    float4 h;
+    short4 l;
+};
+
+__device__ __forceinline__ RawQuad mx_load_raw(const float* hi_row, const short* lo_row) {
+    return RawQuad{__ldg(reinterpret_cast<const float4*>(hi_row)), __ldg(reinterpret_cast<const short4*>(lo_row))};
+}
+
+__device__ __forceinline__ RawQuad zero_raw() { return RawQuad{make_float4(0.f, 0.f, 0.f, 0.f), make_short4(0, 0, 0, 0)}; }
+
+__device__ __forceinline__ void add_raw(Quad& a, const RawQuad& r) {
+    a.v[0] = a.v[0] + mx_decode(r.h.x, r.l.x);
+    a.v[1] = a.v[1] + mx_decode(r.h.y, r.l.y);
+    a.v[2] = a.v[2] + mx_decode(r.h.z, r.l.z);
+    a.v[3] = a.v[3] + mx_decode(r.h.w, r.l.w);
+}
+
+__device__ __forceinline__ Quad mx_load(const float* hi_row, const short* lo_row) {
+    Quad q = zero_quad();
+    add_raw(q, mx_load_raw(hi_row, lo_row));
+    return q;
+}
+
+__device__ __forceinline__ void mx_store(float* hi_row, short* lo_row, const Quad& q) {
+    float4 h;
+    short4 l;
+    mx_encode(q.v[0], h.x, l.x);
+    mx_encode(q.v[1], h.y, l.y);
+    mx_encode(q.v[2], h.z, l.z);
+    mx_encode(q.v[3], h.w, l.w);
+    *reinterpret_cast<float4*>(hi_row) = h;
+    *reinterpret_cast<short4*>(lo_row) = l;
+}
+
+// Columns [c, c + 4) of an FP64 row with columns >= k read as zero.
+__device__ __forceinline__ Quad f64_load_guarded(const double* row, int64_t c, int64_t k) {
+    Quad q;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) q.v[i] = c + i < k ? __ldg(row + c + i) : 0.0;
+    return q;
+}
+
+__device__ __forceinline__ void f64_store_guarded(double* row, int64_t c, int64_t k, const Quad& q) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        if (c + i < k) row[c + i] = q.v[i];
+}
+
+template <int INIT>
+__device__ __forceinline__ Quad mx_init(const LevelArgs& a, int64_t row, int64_t c) {
+    if constexpr (INIT == GRG_B200_INIT_VECTOR) {
+        return f64_load_guarded(static_cast<const double*>(a.init_vector), c, a.k);
+    } else if constexpr (INIT == GRG_B200_INIT_XTX) {
+        const double x = __ldg(static_cast<const double*>(a.xtx_node) + row);
+        return Quad{{x, x, x, x}};
+    } else if constexpr (INIT == GRG_B200_INIT_MATRIX) {
+        const int64_t orig = __ldg(a.node_perm + row);
+        if (a.err && (orig < 0 || orig >= a.lim_state)) {
+            report(a.err, kErrPerm);
+            return zero_quad();
+        }
+        return f64_load_guarded(static_cast<const double*>(a.init_matrix) + orig * a.ld_init, c, a.k);
+    } else {
+        return zero_quad();
+    }
+}
+
+// Encoded row named by a coded entry (hi and lo row starts); false when the entry is skipped.
+__device__ __forceinline__ bool mx_entry(const LevelArgs& a, uint32_t code, const float*& hi, const short*& lo) {
+    const uint32_t src = (code >> GRG_B200_SRC_SHIFT) & GRG_B200_SRC_MASK;
+    const int64_t id = code & GRG_B200_ID_MASK;
+    int64_t off;
+    if (src == GRG_B200_SRC_STATE) {
+        if (a.err && id >= a.lim_state) {
+            report(a.err, kErrStateId);
+            return false;
+        }
+        off = id * a.ld_state;
+        hi = static_cast<const float*>(a.state) + off;
+        lo = static_cast<const short*>(a.state_lo) + off;
+        return true;
+    }
+    if (src == GRG_B200_SRC_INPUT) {
+        if (a.err && id >= a.lim_x) {
+            report(a.err, kErrInputId);
+            return false;
+        }
+        off = id * a.ld_x;
+        hi = static_cast<const float*>(a.x) + off;
+        lo = static_cast<const short*>(a.x_lo) + off;
+        return true;
+    }
+    if (src != GRG_B200_SRC_MISS || !a.use_miss) return false;
+    if (a.err && id >= a.lim_miss) {
+        report(a.err, kErrMissId);
+        return false;
+    }
+    off = id * a.ld_miss;
+    hi = static_cast<const float*>(a.miss) + off;
+    lo = static_cast<const short*>(a.miss_lo) + off;
+    return true;
+}
+
+// Narrow rows of padded lists in mixed storage: the ownership and code prefetch of
+// level_vec_kernel with 4 columns per lane; adds in list order, segment by segment.
+template <int INIT>
+__global__ void __launch_bounds__(kNarrowThreads, 3) level_mx_kernel(LevelArgs a) {
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t pos = ((static_cast<int64_t>(blockIdx.x) * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    if (pos >= narrow) return;
+    const int32_t e0 = __ldg(a.row_ptr + pos);
+    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int64_t row = level_row(a, pos);
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    const int64_t step = static_cast<int64_t>(4) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(glane) * 4; c < a.k; c += step) {
+        Quad acc = mx_init<INIT>(a, row, c);
+        Quad seg = zero_quad();
+        const int32_t q1 = e1 >> 2;
+        int32_t q = e0 >> 2;
+        uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
+        for (; q < q1; ++q) {
+            const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+            const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+            RawQuad val[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const float* hi = nullptr;
+                const short* lo = nullptr;
+                val[u] = mx_entry(a, code[u], hi, lo) ? mx_load_raw(hi + c, lo + c) : zero_raw();
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (code[u] & GRG_B200_SEG_START) {
+                    add_quad(acc, seg);
+                    seg = zero_quad();
+                }
+                add_raw(seg, val[u]);  // skipped entries decode to +0
+            }
+            cur = nxt;
+        }
+        add_quad(acc, seg);
+        const int64_t off = row * a.ld_state + c;
+        mx_store(static_cast<float*>(a.state) + off, static_cast<short*>(a.state_lo) + off, acc);
+    }
+}
+
+// Heavy rows in mixed storage, one warp each (as level_warp_kernel, padded lists).
+template <int INIT>
+__global__ void __launch_bounds__(kWarpRowThreads) level_mx_warp_kernel(LevelArgs a) {
+    const int64_t w = static_cast<int64_t>(blockIdx.x) * (kWarpRowThreads / 32) + (threadIdx.x >> 5);
+    if (w >= a.num_heavy) return;  // warp-uniform
+    const int lane32 = threadIdx.x & 31;
+    const int64_t pos = __ldg(a.heavy_rows + w);
+    const int32_t e0 = __ldg(a.row_ptr + pos);
+    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
+    const int64_t row = level_row(a, pos);
+    const int g_lanes = 1 << a.log2g;
+    const int groups = 32 >> a.log2g;
+    const int glane = lane32 & (g_lanes - 1);
+    const int grp = lane32 >> a.log2g;
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const int64_t step = static_cast<int64_t>(4) << a.log2g;
+    for (int64_t base = 0; base < a.k; base += step) {  // uniform trip count across the warp
+        const int64_t c = base + static_cast<int64_t>(glane) * 4;
+        const bool active = c < a.k;
+        Quad part = zero_quad();
+        if (active) {
+            for (int32_t q = (e0 >> 2) + grp; q < (e1 >> 2); q += groups) {
+                const uint4 cq = __ldg(codes4 + q);
+                const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
+                RawQuad val[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const float* hi = nullptr;
+                    const short* lo = nullptr;
+                    val[u] = mx_entry(a, code[u], hi, lo) ? mx_load_raw(hi + c, lo + c) : zero_raw();
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) add_raw(part, val[u]);
+            }
+        }
+        for (int off = 16; off >= g_lanes; off >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) part.v[i] = part.v[i] + __shfl_xor_sync(kFullMask, part.v[i], off);
+        }
+        if (grp == 0 && active) {
+            Quad acc = mx_init<INIT>(a, row, c);
+            add_quad(acc, part);
+            const int64_t o = row * a.ld_state + c;
+            mx_store(static_cast<float*>(a.state) + o, static_cast<short*>(a.state_lo) + o, acc);
+        }
+    }
+}
+
+// Encoded copy of an FP64 matrix: dst[r, c] = src[r, c] for c < k, 0 for k <= c < ld.
+__global__ void __launch_bounds__(256) mx_encode_rows_kernel(const double* src, int64_t ld_src, int64_t rows, int64_t k,
+                                                             float* dst_hi, short* dst_lo, int64_t ld, int32_t log2g) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t r = t >> log2g;
+    if (r >= rows) return;
+    const int lane = static_cast<int>(t & ((1 << log2g) - 1));
+    for (int64_t c = static_cast<int64_t>(lane) * 4; c < ld; c += static_cast<int64_t>(4) << log2g)
+        mx_store(dst_hi + r * ld + c, dst_lo + r * ld + c, f64_load_guarded(src + r * ld_src, c, k));
+}
+
+// Up seeding of level 0 in mixed storage: state[r] = init(r) (+ input row for samples).
+template <int INIT>
+__global__ void __launch_bounds__(256) seed_up_mx_kernel(LevelArgs a, int64_t num_samples, const int32_t* s2i, int32_t by_ind) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t row = t >> a.log2g;
+    if (row >= a.num_rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    int64_t xrow = row;
+    if (row < num_samples && by_ind) {
+        xrow = __ldg(s2i + row);
+        if (a.err && (xrow < 0 || xrow >= a.lim_x)) {
+            report(a.err, kErrInputId);
+            return;
+        }
+    }
+    const double* x = static_cast<const double*>(a.x);
+    for (int64_t c = static_cast<int64_t>(lane) * 4; c < a.k; c += static_cast<int64_t>(4) << a.log2g) {
+        Quad v = mx_init<INIT>(a, row, c);
+        if (row < num_samples) add_quad(v, f64_load_guarded(x + xrow * a.ld_x, c, a.k));
+        const int64_t o = row * a.ld_state + c;
+        mx_store(static_cast<float*>(a.state) + o, static_cast<short*>(a.state_lo) + o, v);
+    }
+}
+
 constexpr int kWideThreads = 128;
 constexpr int kWideChunk = 512;  // gather-list entries staged per round
 
@@ -584,6 +954,7 @@ struct OutArgs {
     int32_t log2g;
     int32_t* err;
     int64_t lim;
+    const void* state_lo;  // mixed storage only
 };
 
 template <typename T, int V>
@@ -664,6 +1035,78 @@ __global__ void __launch_bounds__(256) emit_all_kernel(OutArgs a) {
         st_pack(out + j * a.ld_out + c, ld_ro<T, V>(state + n * a.ld_state + c));
 }
 
+// Output kernels for mixed storage: decode to FP64, 4 columns per lane, columns >= k skipped.
+__device__ __forceinline__ void mx_apply_bias(const OutArgs& a, int64_t r, int64_t c, Quad& v) {
+    if (a.bias_mode == GRG_B200_BIAS_XTX) {
+        const double b = __ldg(static_cast<const double*>(a.bias) + r);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v.v[i] = __dadd_rn(v.v[i], b);
+    } else if (a.bias_mode == GRG_B200_BIAS_VECTOR) {
+        const double b = __ldg(static_cast<const double*>(a.bias) + r);
+        const Quad iv = f64_load_guarded(static_cast<const double*>(a.init_vector), c, a.k);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v.v[i] = __dadd_rn(v.v[i], __dmul_rn(b, iv.v[i]));
+    }
+}
+
+__device__ __forceinline__ Quad mx_state_row(const OutArgs& a, int64_t n, int64_t c) {
+    const int64_t o = n * a.ld_state + c;
+    return mx_load(static_cast<const float*>(a.state) + o, static_cast<const short*>(a.state_lo) + o);
+}
+
+template <bool BIAS_PER_ENTRY>
+__global__ void __launch_bounds__(256) gather_out_mx_kernel(OutArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t r = t >> a.log2g;
+    if (r >= a.rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    const int32_t e0 = __ldg(a.ptr + r), e1 = __ldg(a.ptr + r + 1);
+    double* out = static_cast<double*>(a.out);
+    for (int64_t c = static_cast<int64_t>(lane) * 4; c < a.k; c += static_cast<int64_t>(4) << a.log2g) {
+        Quad s = zero_quad();
+        for (int32_t e = e0; e < e1; ++e) {
+            const int64_t n = __ldg(a.idx + e);
+            if (a.err && (n < 0 || n >= a.lim)) {
+                report(a.err, kErrSelector);
+                continue;
+            }
+            Quad v = mx_state_row(a, n, c);
+            if constexpr (BIAS_PER_ENTRY) mx_apply_bias(a, n, c, v);
+            add_quad(s, v);
+        }
+        if constexpr (!BIAS_PER_ENTRY) mx_apply_bias(a, r, c, s);
+        f64_store_guarded(out + r * a.ld_out, c, a.k, s);
+    }
+}
+
+__global__ void __launch_bounds__(256) copy_out_mx_kernel(OutArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t r = t >> a.log2g;
+    if (r >= a.rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    double* out = static_cast<double*>(a.out);
+    for (int64_t c = static_cast<int64_t>(lane) * 4; c < a.k; c += static_cast<int64_t>(4) << a.log2g) {
+        Quad v = mx_state_row(a, r, c);
+        mx_apply_bias(a, r, c, v);
+        f64_store_guarded(out + r * a.ld_out, c, a.k, v);
+    }
+}
+
+__global__ void __launch_bounds__(256) emit_all_mx_kernel(OutArgs a) {
+    const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int64_t j = t >> a.log2g;
+    if (j >= a.rows) return;
+    const int lane = static_cast<int>(t & ((1 << a.log2g) - 1));
+    const int64_t n = __ldg(a.idx + j);
+    if (a.err && (n < 0 || n >= a.lim)) {
+        report(a.err, kErrPerm);
+        return;
+    }
+    double* out = static_cast<double*>(a.out);
+    for (int64_t c = static_cast<int64_t>(lane) * 4; c < a.k; c += static_cast<int64_t>(4) << a.log2g)
+        f64_store_guarded(out + j * a.ld_out, c, a.k, mx_state_row(a, n, c));
+}
+
 // ---------------------------------------------------------------------------------------
 // Host-side launch helpers
 // ---------------------------------------------------------------------------------------
@@ -675,6 +1118,12 @@ struct Shape {
 bool aligned(const void* p, int bytes) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) % bytes) == 0; }
 
 Shape choose_shape(const grg_b200_traverse_args* a) {
+    if (a->dtype == GRG_B200_MIXED) {  // 4 columns per lane (16-byte hi + 8-byte lo loads)
+        const int64_t cols = (a->k + 3) / 4;
+        int log2g = 0;
+        while ((1 << log2g) < cols && log2g < 5) ++log2g;
+        return {4, log2g};
+    }
     const int esize = a->dtype == GRG_B200_F64 ? 8 : 4;
     const int64_t lds[] = {a->ld_state, a->ld_input, a->ld_output, a->use_miss ? a->ld_miss : 0, a->ld_init};
     const void* ptrs[] = {a->state, a->input, a->output, a->use_miss ? a->miss : nullptr, a->init_vector, a->init_matrix};
@@ -703,7 +1152,19 @@ dim3 grid_for(int64_t rows, int log2g, int threads) {
 
 int validate_common(const grg_b200_traverse_args* a) {
     if (!a) return fail(GRG_B200_ERR_INVALID, "args is NULL");
-    if (a->dtype != GRG_B200_F64 && a->dtype != GRG_B200_F32) return fail(GRG_B200_ERR_INVALID, "unknown dtype %d", a->dtype);
+    if (a->dtype != GRG_B200_F64 && a->dtype != GRG_B200_F32 && a->dtype != GRG_B200_MIXED)
+        return fail(GRG_B200_ERR_INVALID, "unknown dtype %d", a->dtype);
+    if (a->dtype == GRG_B200_MIXED) {
+        if (a->ld_state % 4 != 0 || !aligned(a->state, 16))
+            return fail(GRG_B200_ERR_INVALID, "mixed state needs ld_state %% 4 == 0 and a 16-byte aligned base");
+        if (a->exact_order) return fail(GRG_B200_ERR_UNSUPPORTED, "mixed storage has no exact-order mode");
+        if (a->direction == GRG_B200_DOWN) {
+            const int64_t need = GRG_B200_MIX_BYTES(a->num_mutations, a->ld_state) * (a->use_miss ? 2 : 1);
+            if (!a->mix_scratch || !aligned(a->mix_scratch, 16) || a->mix_scratch_bytes < need)
+                return fail(GRG_B200_ERR_INVALID, "mixed down needs a 16-byte aligned mix_scratch of %lld bytes (got %lld)",
+                            (long long)need, (long long)a->mix_scratch_bytes);
+        }
+    }
     if (a->k < 1) return fail(GRG_B200_ERR_INVALID, "k must be >= 1, got %lld", (long long)a->k);
     if (a->ld_state < a->k) return fail(GRG_B200_ERR_INVALID, "ld_state %lld < k %lld", (long long)a->ld_state, (long long)a->k);
     if (!a->state) return fail(GRG_B200_ERR_INVALID, "state is NULL");
@@ -712,6 +1173,7 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
     if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
+    if (a->heavy_variant < 0 || a->heavy_variant > 1) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 1]", a->heavy_variant);
     if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
     if (a->init_mode == GRG_B200_INIT_XTX && !a->xtx_node) return fail(GRG_B200_ERR_INVALID, "xtx_node is NULL");
     if (a->init_mode == GRG_B200_INIT_MATRIX && (!a->init_matrix || !a->node_perm || a->ld_init < a->k))
@@ -742,11 +1204,25 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
     la.lim_state = a->num_nodes;
     la.lim_x = a->direction == GRG_B200_UP ? (a->by_individual ? a->num_individuals : a->num_samples) : a->num_mutations;
     la.lim_miss = a->num_mutations;
+    if (a->dtype == GRG_B200_MIXED) {
+        la.state_lo = static_cast<char*>(a->state) + GRG_B200_MIX_PLANE(a->num_nodes * a->ld_state * 4);
+        if (a->direction == GRG_B200_DOWN) {  // levels read the encoded copies in mix_scratch
+            char* base = static_cast<char*>(a->mix_scratch);
+            const int64_t hi_bytes = GRG_B200_MIX_PLANE(a->num_mutations * a->ld_state * 4);
+            const int64_t one = GRG_B200_MIX_BYTES(a->num_mutations, a->ld_state);
+            la.x = base;
+            la.x_lo = base + hi_bytes;
+            la.ld_x = a->ld_state;
+            la.miss = base + one;
+            la.miss_lo = base + one + hi_bytes;
+            la.ld_miss = a->ld_state;
+        }
+    }
     return la;
 }
 
 template <typename T, int V>
-int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, cudaStream_t s) {
+int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     if (narrow > 0 && variant == 6) {
         const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
@@ -790,7 +1266,17 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
 #undef GRG_NARROW
         GRG_LAUNCH_CHECK("level_narrow_kernel");
     }
-    if (la.num_heavy > 0) {
+    if (la.num_heavy > 0 && !exact && heavy_variant == 1) {
+        constexpr int rows_per_cta = kWarpRowThreads / 32;
+        const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
+        switch (init_mode) {
+            case 0: level_warp_kernel<T, V, 0><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 1: level_warp_kernel<T, V, 1><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 2: level_warp_kernel<T, V, 2><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            default: level_warp_kernel<T, V, 3><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+        }
+        GRG_LAUNCH_CHECK("level_warp_kernel");
+    } else if (la.num_heavy > 0) {
         const dim3 grid(static_cast<unsigned>(la.num_heavy));
 #define GRG_WIDE(INIT)                                                                            \
     if (exact) level_wide_kernel<T, V, INIT, true><<<grid, kWideThreads, 0, s>>>(la);            \
@@ -803,6 +1289,33 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         }
 #undef GRG_WIDE
         GRG_LAUNCH_CHECK("level_wide_kernel");
+    }
+    return GRG_B200_OK;
+}
+
+int launch_level_mx(const LevelArgs& la, int init_mode, cudaStream_t s) {
+    const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
+    if (narrow > 0) {
+        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
+        switch (init_mode) {
+            case 0: level_mx_kernel<0><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 1: level_mx_kernel<1><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 2: level_mx_kernel<2><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            default: level_mx_kernel<3><<<grid, kNarrowThreads, 0, s>>>(la); break;
+        }
+        GRG_LAUNCH_CHECK("level_mx_kernel");
+    }
+    if (la.num_heavy > 0) {
+        constexpr int rows_per_cta = kWarpRowThreads / 32;
+        const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
+        switch (init_mode) {
+            case 0: level_mx_warp_kernel<0><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 1: level_mx_warp_kernel<1><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 2: level_mx_warp_kernel<2><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            default: level_mx_warp_kernel<3><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+        }
+        GRG_LAUNCH_CHECK("level_mx_warp_kernel");
     }
     return GRG_B200_OK;
 }
@@ -835,15 +1348,16 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     la.heavy_rows = reinterpret_cast<const int32_t*>(base + L->off_heavy);
     la.row_ids = L->off_row_ids >= 0 ? reinterpret_cast<const int32_t*>(base + L->off_row_ids) : nullptr;
     if (L->list_align != 1 && L->list_align != 4) return fail(GRG_B200_ERR_INVALID, "list_align must be 1 or 4, got %d", L->list_align);
-    if (a->narrow_variant == 6 && L->list_align != 4)
-        return fail(GRG_B200_ERR_INVALID, "narrow_variant 6 needs padded gather lists (list_align 4)");
+    if ((a->narrow_variant == 6 || a->dtype == GRG_B200_MIXED) && L->list_align != 4)
+        return fail(GRG_B200_ERR_INVALID, "narrow_variant 6 and mixed storage need padded gather lists (list_align 4)");
     if (L->list_align == 4 && (L->off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
     la.list_align = L->list_align;
     la.num_heavy = L->num_heavy;
     la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
     const bool exact = a->exact_order != 0;
+    if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, s);
     return dispatch(a, sh, [&](auto t, auto v) {
-        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, s);
+        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant, s);
     });
 }
 
@@ -855,6 +1369,16 @@ int seed_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t 
     la.row_begin = 0;
     la.num_rows = a->level0_rows;
     const dim3 grid = grid_for(la.num_rows, la.log2g, 256);
+    if (a->dtype == GRG_B200_MIXED) {
+        switch (a->init_mode) {
+            case 0: seed_up_mx_kernel<0><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            case 1: seed_up_mx_kernel<1><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            case 2: seed_up_mx_kernel<2><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            default: seed_up_mx_kernel<3><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+        }
+        GRG_LAUNCH_CHECK("seed_up_mx_kernel");
+        return (int)GRG_B200_OK;
+    }
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
@@ -882,6 +1406,8 @@ OutArgs out_args(const grg_b200_traverse_args* a, const Shape& sh) {
     o.log2g = sh.log2g;
     o.err = a->error_word;
     o.lim = a->num_nodes;
+    if (a->dtype == GRG_B200_MIXED)
+        o.state_lo = static_cast<const char*>(a->state) + GRG_B200_MIX_PLANE(a->num_nodes * a->ld_state * 4);
     return o;
 }
 
@@ -895,6 +1421,21 @@ int output_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_
     o.ptr = a->sel_mut_ptr;
     o.idx = a->sel_mut_idx;
     const dim3 grid = grid_for(o.rows, o.log2g, 256);
+    if (a->dtype == GRG_B200_MIXED) {
+        gather_out_mx_kernel<false><<<grid, 256, 0, s>>>(o);
+        GRG_LAUNCH_CHECK("gather_out_mx_kernel(sel_mut)");
+        if (a->use_miss) {
+            OutArgs m = o;
+            m.ptr = a->sel_miss_ptr;
+            m.idx = a->sel_miss_idx;
+            m.out = a->miss;
+            m.ld_out = a->ld_miss;
+            m.bias_mode = GRG_B200_BIAS_NONE;
+            gather_out_mx_kernel<false><<<grid, 256, 0, s>>>(m);
+            GRG_LAUNCH_CHECK("gather_out_mx_kernel(sel_miss)");
+        }
+        return (int)GRG_B200_OK;
+    }
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
@@ -928,6 +1469,12 @@ int output_down_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStrea
     }
     if (o.rows == 0) return GRG_B200_OK;
     const dim3 grid = grid_for(o.rows, o.log2g, 256);
+    if (a->dtype == GRG_B200_MIXED) {
+        if (a->by_individual) gather_out_mx_kernel<true><<<grid, 256, 0, s>>>(o);
+        else copy_out_mx_kernel<<<grid, 256, 0, s>>>(o);
+        GRG_LAUNCH_CHECK("output_down_mx");
+        return (int)GRG_B200_OK;
+    }
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
@@ -944,6 +1491,11 @@ int emit_all_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t
     o.rows = a->num_nodes;
     o.idx = a->inv_node_perm;
     const dim3 grid = grid_for(o.rows, o.log2g, 256);
+    if (a->dtype == GRG_B200_MIXED) {
+        emit_all_mx_kernel<<<grid, 256, 0, s>>>(o);
+        GRG_LAUNCH_CHECK("emit_all_mx_kernel");
+        return (int)GRG_B200_OK;
+    }
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
@@ -951,6 +1503,27 @@ int emit_all_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t
         GRG_LAUNCH_CHECK("emit_all_kernel");
         return (int)GRG_B200_OK;
     });
+}
+
+// Mixed down: encoded copies of the input (and miss) rows, which the level lists read.
+int encode_down_inputs(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    if (a->num_mutations == 0) return GRG_B200_OK;
+    const LevelArgs la = level_args(a, sh);
+    const int64_t ld = a->ld_state;
+    int log2g = 0;
+    while ((1 << log2g) < (ld + 3) / 4 && log2g < 5) ++log2g;
+    const dim3 grid = grid_for(a->num_mutations, log2g, 256);
+    mx_encode_rows_kernel<<<grid, 256, 0, s>>>(static_cast<const double*>(a->input), a->ld_input, a->num_mutations, a->k,
+                                               static_cast<float*>(const_cast<void*>(la.x)),
+                                               static_cast<short*>(const_cast<void*>(la.x_lo)), ld, log2g);
+    GRG_LAUNCH_CHECK("mx_encode_rows_kernel(input)");
+    if (a->use_miss) {
+        mx_encode_rows_kernel<<<grid, 256, 0, s>>>(static_cast<const double*>(a->miss), a->ld_miss, a->num_mutations, a->k,
+                                                   static_cast<float*>(const_cast<void*>(la.miss)),
+                                                   static_cast<short*>(const_cast<void*>(la.miss_lo)), ld, log2g);
+        GRG_LAUNCH_CHECK("mx_encode_rows_kernel(miss)");
+    }
+    return GRG_B200_OK;
 }
 
 }  // namespace
@@ -1082,6 +1655,9 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
     if (a->direction == GRG_B200_UP) {
         rc = seed_up_impl(a, sh, s);
         if (rc) return rc;
+    } else if (a->dtype == GRG_B200_MIXED) {
+        rc = encode_down_inputs(a, sh, s);
+        if (rc) return rc;
     }
     // Fork the copy stream off the caller's stream so streamed copies are ordered after the
     // caller's earlier work (and join a CUDA graph capture in progress).
@@ -1159,6 +1735,7 @@ int static_state_address(void** out) {
 int grg_b200_traverse_static(const grg_b200_traverse_args* a, void* stream_handle) {
     if (!a) return fail(GRG_B200_ERR_INVALID, "args is NULL");
     if (a->k < 1) return fail(GRG_B200_ERR_INVALID, "k must be >= 1, got %lld", (long long)a->k);
+    if (a->dtype == GRG_B200_MIXED) return fail(GRG_B200_ERR_UNSUPPORTED, "grg_b200_traverse_static serves the FP64 and FP32 dtypes only");
     const int64_t esize = a->dtype == GRG_B200_F64 ? 8 : 4;
     if (a->num_nodes < 0 || a->num_nodes > (int64_t)GRG_B200_STATIC_STATE_BYTES / esize / a->k)
         return fail(GRG_B200_ERR_UNSUPPORTED,

@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 4
+#define GRG_B200_ABI_VERSION 6
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -64,7 +64,21 @@ typedef enum grg_b200_status {
     GRG_B200_ERR_UNSUPPORTED = 3  /* valid request outside this build's limits */
 } grg_b200_status;
 
-typedef enum grg_b200_dtype { GRG_B200_F64 = 0, GRG_B200_F32 = 1 } grg_b200_dtype;
+/*
+ * GRG_B200_MIXED: input, output, miss and init buffers are FP64; the node state (and, for
+ * down, encoded copies of input and miss in mix_scratch) is stored in 6 bytes per value:
+ * hi = the value rounded to FP32 and lo = a 16-bit correction in units of 2^(e(hi) - 39), so
+ * a stored value is within 2^-40 of the exact one relative to |hi| (integers below 2^40 are
+ * exact).  Sums are accumulated in FP64 and rounded back once per node.  A mixed buffer of
+ * R rows and ld columns (ld a multiple of 4) is float hi[R * ld] followed by int16
+ * lo[R * ld]; see GRG_B200_MIX_BYTES.  Mixed traversals never use exact order.
+ */
+typedef enum grg_b200_dtype { GRG_B200_F64 = 0, GRG_B200_F32 = 1, GRG_B200_MIXED = 2 } grg_b200_dtype;
+
+/* Bytes of one mixed buffer of `rows` rows and `ld` columns (each plane rounded up to 16). */
+#define GRG_B200_MIX_PLANE(bytes) ((((bytes) + 15) / 16) * 16)
+#define GRG_B200_MIX_BYTES(rows, ld) \
+    (GRG_B200_MIX_PLANE((int64_t)(rows) * (ld) * 4) + GRG_B200_MIX_PLANE((int64_t)(rows) * (ld) * 2))
 typedef enum grg_b200_direction { GRG_B200_UP = 0, GRG_B200_DOWN = 1 } grg_b200_direction;
 typedef enum grg_b200_init {
     GRG_B200_INIT_NONE = 0,
@@ -176,6 +190,14 @@ typedef struct grg_b200_traverse_args {
                                            per thread (8 CTAs per SM); 6: padded lists (list_align
                                            4) read 4 codes per 16-byte load, next 4 prefetched
                                            while the current 4 rows load. */
+    int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
+                                           (list staged in shared memory, tree reduction); 1 one
+                                           warp per row (lane groups split the list, shuffle
+                                           reduction).  Exact order always uses one CTA per row. */
+    void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
+                                           (use_miss) the encoded miss rows, each a mixed buffer of
+                                           num_mutations rows and ld_state columns */
+    int64_t mix_scratch_bytes;
 } grg_b200_traverse_args;
 
 #define GRG_B200_NARROW_VARIANTS 7

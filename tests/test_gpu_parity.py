@@ -23,16 +23,17 @@ def _req(k=8, **kw):
 
 
 def _layout(paths, *, dtype=np.float64, req=None, exact=False, heavy=None, budget=0, ring=0, allow_residency=True, stream=0,
-            pair=None, variant=0):
+            pair=None, variant=0, heavy_variant=None, precision="plain"):
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, plan_b200_layout
 
     if pair is None:
-        kw = {"narrow_variant": variant}
+        kw = {"narrow_variant": variant, "heavy_variant": heavy_variant}
         if heavy is not None:
             kw["heavy_threshold"] = heavy
         pair = B200PlanPair(plan_up=B200Plan(exact_order=exact, **kw), plan_down=B200Plan(exact_order=exact, **kw))
     return plan_b200_layout(artifacts=list(paths), dtype=dtype, requirements=req or _req(), vram_budget_bytes=budget,
-                            ring_buffer_size=ring, allow_residency=allow_residency, device=0, stream=stream, pair=pair)
+                            ring_buffer_size=ring, allow_residency=allow_residency, device=0, stream=stream, pair=pair,
+                            precision=precision)
 
 
 def _run_case(grg, case, data):
@@ -74,13 +75,15 @@ def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
         assert runtime.device_error() == 0
 
 
+@pytest.mark.parametrize("heavy_variant", [0, 1])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
-def test_golden_fast_mode_heavy_rows(group, golden_data):
-    """Default (tree-reduced heavy rows): exact for integer-valued inputs, tolerance otherwise."""
+def test_golden_fast_mode_heavy_rows(group, heavy_variant, golden_data):
+    """Default mode with split heavy rows (one CTA or one warp per row, fixed-order
+    reductions): exact for integer-valued inputs, tolerance otherwise."""
     from grg_spmv_b200.backends.b200 import B200Runtime
 
     name, dtype = group
-    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=False, heavy=2)
+    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=False, heavy=2, heavy_variant=heavy_variant)
     rtol, atol = (RTOL_F64, ATOL_F64) if dtype == "float64" else (RTOL_F32, ATOL_F32)
     with B200Runtime(layout, check_bounds=True) as runtime:
         (grg,) = runtime.grgs
@@ -92,4 +95,34 @@ def test_golden_fast_mode_heavy_rows(group, golden_data):
                 np.testing.assert_array_equal(out, expected, err_msg=case["key"])
             else:
                 np.testing.assert_allclose(out, expected, rtol=rtol, atol=atol * max(1.0, np.abs(expected).max()), err_msg=case["key"])
+        assert runtime.device_error() == 0
+
+
+MIXED_RTOL = 1e-10  # mixed precision: max |got - ref| / max |ref| per result
+
+
+@pytest.mark.parametrize("heavy", [128, 2], ids=["narrow", "heavy-rows"])
+@pytest.mark.parametrize("group", [g for g in sorted(GROUPS) if g[1] == "float64"], ids=lambda g: g[0])
+def test_golden_mixed_precision(group, heavy, golden_data):
+    """Mixed precision (6-byte node state, FP64 sums) against the reference's FP64 golden
+    outputs: integer-valued inputs without a real-valued init are exact, everything else is
+    within MIXED_RTOL of the largest output magnitude."""
+    from grg_spmv_b200.backends.b200 import B200Runtime
+
+    name, dtype = group
+    layout = _layout([artifact_path(name)], dtype=np.float64, exact=False, heavy=heavy, variant=6, precision="mixed")
+    with B200Runtime(layout, check_bounds=True) as runtime:
+        (grg,) = runtime.grgs
+        for case in GROUPS[group]:
+            out, miss = _run_case(grg, case, golden_data)
+            expected = golden_data[case["key"] + "|out"]
+            assert out.dtype == np.float64
+            integer = any(tag in case["case"] for tag in ("pm1", "ones", "zeros"))
+            if integer and case["init"] is None:
+                np.testing.assert_array_equal(out, expected, err_msg=case["key"])
+            else:
+                scale = max(float(np.abs(expected).max()), 1e-300)
+                assert float(np.abs(out - expected).max()) <= MIXED_RTOL * scale, case["key"]
+            if case["miss"] and case["direction"] == "up" and integer:
+                np.testing.assert_array_equal(miss, golden_data[case["key"] + "|miss_out"], err_msg=case["key"])
         assert runtime.device_error() == 0

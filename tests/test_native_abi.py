@@ -80,3 +80,21 @@ def test_ring_create_rejects_bad_sizes():
     lib = nat.load_library()
     ring = ctypes.c_void_p()
     assert lib.grg_b200_ring_create(0, 0, ctypes.byref(ring)) == nat.ERR_INVALID
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
+def test_mixed_storage_sizes_match_c(tmp_path):
+    """The Python sizes of mixed buffers equal GRG_B200_MIX_BYTES (the runtime allocates with them)."""
+    cases = [(1, 4), (3, 4), (5, 8), (1000, 12), (999_983, 36)]
+    src = tmp_path / "mix.c"
+    lines = ["#include <stdio.h>", '#include "grg_b200.h"', "int main(void) {",
+             '  printf("%d\\n", (int)GRG_B200_MIXED);']
+    lines += [f'  printf("%lld\\n", (long long)GRG_B200_MIX_BYTES({r}, {ld}));' for r, ld in cases]
+    lines += ["  return 0;", "}"]
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "mix"
+    subprocess.run(["gcc", f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert out[0] == nat.MIXED
+    assert out[1:] == [nat.mix_bytes(r, ld) for r, ld in cases]
+    assert [nat.mix_ld(k) for k in (1, 3, 4, 5, 32, 33)] == [4, 4, 4, 8, 32, 36]

@@ -20,12 +20,12 @@ def _req(k=2, **kw):
     return RuntimeRequirements(**base)
 
 
-def _plan(names=("band3",), *, budget=0, ring=0, allow=True, pair=None, req=None, dtype=np.float64):
+def _plan(names=("band3",), *, budget=0, ring=0, allow=True, pair=None, req=None, dtype=np.float64, precision="plain"):
     paths = tuple(artifact_path(n) for n in names)
     return plan_layout_from_scans(scans=tuple(scan_grg_spmv(p) for p in paths), paths=paths, dtype=dtype,
                                   requirements=req or _req(), requested_budget=budget, requested_ring=ring,
                                   allow_residency=allow, device_id=0, stream_ptr=0, stream_owner=None,
-                                  pair=pair or B200PlanPair())
+                                  pair=pair or B200PlanPair(), precision=precision)
 
 
 def _keys(layout, resident: bool):
@@ -101,6 +101,9 @@ def test_plan_options_validate():
         B200Plan.from_dict({"exact_order": True, "bogus": 1})
     with pytest.raises(ValueError):
         B200PlanPair(plan_up=None, plan_down=None)
+    with pytest.raises(ValueError):
+        B200Plan(heavy_variant=2)
+    assert B200Plan.from_dict({"heavy_variant": 1}).heavy_variant == 1
     assert B200Plan().locality(Direction.DOWN) and not B200Plan().locality(Direction.UP)
 
 
@@ -109,6 +112,31 @@ def test_float32_halves_dense_bytes():
     f32 = _plan(dtype=np.float32)
     assert f32.bytes_by_category["state"] * 2 == f64.bytes_by_category["state"]
     assert f32.bytes_by_category["resident_sparse"] == f64.bytes_by_category["resident_sparse"]
+
+
+def test_mixed_precision_state_and_scratch_bytes():
+    from grg_spmv_b200.backends.b200 import _native as nat
+
+    req = _req()
+    f64 = _plan(req=req)
+    mixed = _plan(req=req, precision="mixed")
+    k = max(req.max_k_up, req.max_k_down)
+    assert mixed.precision == "mixed" and f64.precision == "plain"
+    assert mixed.bytes_by_category["state"] == nat.mix_bytes(mixed.max_num_nodes, nat.mix_ld(k))
+    assert mixed.mix_scratch_bytes == nat.mix_bytes(mixed.max_num_mutations, nat.mix_ld(k)) * (2 if req.need_down_miss_input else 1)
+    assert mixed.bytes_by_category["scratch"] == 256 + mixed.mix_scratch_bytes
+    assert mixed.bytes_by_category["resident_sparse"] == f64.bytes_by_category["resident_sparse"]
+
+
+def test_mixed_precision_rejects_incompatible_options():
+    with pytest.raises(ValueError, match="precision"):
+        _plan(precision="half")
+    with pytest.raises(ValueError, match="float64"):
+        _plan(dtype=np.float32, precision="mixed")
+    with pytest.raises(ValueError, match="exact_order"):
+        _plan(precision="mixed", pair=B200PlanPair(plan_up=B200Plan(exact_order=True)))
+    with pytest.raises(ValueError, match="pad_lists"):
+        _plan(precision="mixed", pair=B200PlanPair(plan_down=B200Plan(pad_lists=False, narrow_variant=5)))
 
 
 @pytest.mark.parametrize("heavy", [1, 2, 128])
