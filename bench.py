@@ -56,6 +56,10 @@ def parse_args():
     p.add_argument("--exact-order", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-tiers", action="store_true",
+                   help="skip the batched / mixed-precision comparison on uneven RHS blocks (runs at N=1 only)")
+    p.add_argument("--tier-blocks", default="1,3,16,64,256", help="RHS block widths of the tier comparison")
+    p.add_argument("--tier-steps", type=int, default=3)
     p.add_argument("--no-clocks", action="store_true", help="skip clock sampling and its untimed busy loops")
     p.add_argument("--artifact", default=None, help=".grg_spmv to use (generated there first if missing)")
     p.add_argument("--heavy-threshold", type=int, default=None)
@@ -63,7 +67,12 @@ def parse_args():
     p.add_argument("--no-graphs", action="store_true", help="launch kernels per level instead of replaying a CUDA graph")
     p.add_argument("--no-balance", action="store_true", help="do not group narrow rows by length")
     p.add_argument("--autotune", action="store_true", help="pick the narrow and heavy kernels per direction at runtime entry")
-    p.add_argument("--heavy-variant", type=int, default=None, help="heavy-row kernel: 0 CTA per row, 1 warp per row")
+    p.add_argument("--heavy-variant", type=int, default=None,
+                   help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
+    p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
+    p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
+    p.add_argument("--precision", choices=["plain", "mixed"], default="plain",
+                   help="node state in FP64 (plain) or FP32 + 16-bit correction with FP64 sums (mixed)")
     p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
     p.add_argument("--row-order-down", choices=["natural", "locality"], default=None)
     return p.parse_args()
@@ -209,11 +218,15 @@ def run_b200(args) -> None:
         extra["autotune"] = True
     if args.heavy_variant is not None:
         extra["heavy_variant"] = args.heavy_variant
+    if args.short_first:
+        extra["long_first"] = False
+    if args.narrow_split is not None:
+        extra["narrow_split"] = args.narrow_split
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
                         plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
     stream = torch.cuda.Stream(device=device)
     layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
-                              device=local_rank, stream=stream, pair=pair)
+                              device=local_rank, stream=stream, pair=pair, precision=args.precision)
     t0 = time.perf_counter()
     runtime = B200Runtime(layout, use_graphs=not args.no_graphs).__enter__()
     enter_s = time.perf_counter() - t0
@@ -276,6 +289,7 @@ def run_b200(args) -> None:
     value = total_work / (max_ms / 1e3)
 
     # Live per-kernel timing of the level gathers (one instrumented up+down pass).
+    vb = 8 if args.precision == "plain" else 6  # bytes per stored node value
     lib = runtime._lib
     level_ms = {"up": 0.0, "down": 0.0}
     level_launches = 0
@@ -299,7 +313,8 @@ def run_b200(args) -> None:
                                                       ctypes.c_void_p(stream.cuda_stream)), "run_level")
                 b.record(stream)
                 evs.append((a, b))
-                level_launches += 1 + (1 if levels.array[i].num_heavy > 0 else 0)
+                fused = op._args.heavy_variant == 2 and op._args.narrow_variant == 6 and not op._args.exact_order
+                level_launches += 1 + (1 if levels.array[i].num_heavy > 0 and not fused else 0)
             if name == "up":
                 nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
             else:
@@ -312,10 +327,10 @@ def run_b200(args) -> None:
             level_ms[name] = sum(a.elapsed_time(b) for a, b in evs)
             for (a, b), lv, unit in zip(evs, lvs, units):
                 ms = a.elapsed_time(b)
-                nbytes = level_bytes([unit], k, 8, "up", M, False)
+                nbytes = level_bytes([unit], k, vb, "up", M, False)
                 print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
-            lv_bytes += level_bytes(units, k, 8, name, M, use_miss=True)
+            lv_bytes += level_bytes(units, k, vb, name, M, use_miss=True)
     launches_per_step = level_launches + 1 + 1 + 1  # + seed_up + output_up + output_down
     level_total_ms = level_ms["up"] + level_ms["down"]
     peak, peak_kind = measured_peak_hbm()
@@ -381,6 +396,11 @@ def run_b200(args) -> None:
     tuned = {d.value: [v, runtime._heavy_variant.get(d)] for d, v in runtime._variant.items()}
     heavy_used = {"up": int(up._args.heavy_variant), "down": int(down._args.heavy_variant)}
     runtime.__exit__(None, None, None)
+    del up, down, runtime
+    torch.cuda.empty_cache()
+    tiers = None
+    if world == 1 and not args.no_tiers:
+        tiers = measure_tiers(args, path, device, stream)
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -393,14 +413,15 @@ def run_b200(args) -> None:
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64",
+            "dtype": "f64" if args.precision == "plain" else "f64 sums, f32+i16 node state",
             "data": "synthetic (seeded generator with the configuration's shapes; no public GRG dataset offline)",
             "config": {"workload": f"{args.workload}: S={S}, levels={scan.num_levels}, N={grg.num_nodes}, E={E}, M={M}, "
                                    f"1% missing, fully resident, up+down per step",
-                       "k": k, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
+                       "k": k, "precision": args.precision, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": pair.plan_down.narrow_variant,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
+                       "long_first": pair.plan_down.long_first, "narrow_split": pair.plan_down.narrow_split,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
@@ -414,11 +435,110 @@ def run_b200(args) -> None:
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "max_rel_err_vs_oracle": max_rel,
+            "tiers": tiers,
             "setup_s": {"generate": gen_s, "runtime_enter": enter_s},
         }
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def measure_tiers(args, path, device, stream) -> dict:
+    """Uneven RHS blocks on the same graph, three ways, same work (sum of blocks, up and down):
+    the plain FP64 drop-in (one prepared op per block and direction, one after another), a
+    plain FP64 batch (one CUDA graph, merged and tiled, autotuned) and a mixed-precision batch.
+    Device time with CUDA events; errors of each batch against the FP64 drop-in's outputs and,
+    for the blocks of width <= 3, against the CPU oracle."""
+    import torch
+
+    from grg_spmv_b200 import RuntimeRequirements
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+
+    blocks = [int(b) for b in args.tier_blocks.split(",") if b]
+    kmax = max(blocks)
+    req = RuntimeRequirements(max_k_up=kmax, max_k_down=kmax, need_down_miss_input=True, need_up_miss_output=False,
+                              need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
+    layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
+                              device=device.index or 0, stream=stream)
+    rng = np.random.default_rng(7)
+    rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(float(np.max(np.abs(ref))), 1e-300))
+    out = {"blocks": blocks, "steps": args.tier_steps, "warmup": max(args.warmup, 3)}
+    with B200Runtime(layout) as rt, torch.cuda.device(device), torch.cuda.stream(stream):
+        (g,) = rt.grgs
+        E = g.num_edges
+        items = [(g, "up", kb) for kb in blocks] + [(g, "down", kb, True) for kb in blocks]
+        xs, misses = [], []
+        for it in items:
+            cols = g.num_samples if it[1] == "up" else g.num_mutations
+            xs.append(torch.from_numpy(rng.standard_normal((it[2], cols))).to(device))
+            misses.append(torch.from_numpy(rng.standard_normal((it[2], g.num_mutations))).to(device) if it[1] == "down" else None)
+        work = 2.0 * E * sum(blocks)
+
+        def timed(step) -> float:
+            for _ in range(max(args.warmup, 3)):
+                step()
+            torch.cuda.synchronize(device)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(args.tier_steps):
+                step()
+            b.record(stream)
+            torch.cuda.synchronize(device)
+            return a.elapsed_time(b) / args.tier_steps
+
+        # 1) plain FP64 drop-in: one prepared op per block and direction.
+        ops = [g.prepare_matmul_cuda(direction=it[1], k=it[2], use_miss=it[1] == "down") for it in items]
+        plain_out = [None] * len(items)
+
+        def dropin_step(keep=False):
+            for i, op in enumerate(ops):
+                op.input.copy_(xs[i])
+                if misses[i] is not None:
+                    op.miss_input.copy_(misses[i])
+                op()
+                if keep:
+                    plain_out[i] = op.output.cpu().numpy()
+
+        ms = timed(dropin_step)
+        dropin_step(keep=True)
+        out["plain_f64_dropin"] = {"value": work / (ms / 1e3), "ms_per_step": ms, "launch": "one prepared op per block"}
+        del ops
+        # 2) and 3) batches.
+        for name, precision in (("plain_f64_batched", "plain"), ("mixed_batched", "mixed")):
+            with rt.prepare_batch(items, precision=precision, autotune=True) as batch:
+                def batch_step():
+                    for i in range(len(items)):
+                        batch.inputs[i].copy_(xs[i])
+                        if misses[i] is not None:
+                            batch.miss_inputs[i].copy_(misses[i])
+                    batch()
+
+                ms_b = timed(batch_step)
+                batch_step()
+                torch.cuda.synchronize(device)
+                errs = [rel(batch.outputs[i].cpu().numpy(), plain_out[i]) for i in range(len(items))]
+                out[name] = {"value": work / (ms_b / 1e3), "ms_per_step": ms_b, "tile_k": batch.tile_k,
+                             "tiles": batch.num_tiles, "tuned_ms": {str(k): v for k, v in batch.tuned_ms.items()},
+                             "max_rel_err_vs_plain_f64": max(errs), "speedup_vs_dropin": ms / ms_b}
+                small = [i for i, it in enumerate(items) if it[2] <= 3]
+                if small and not args.no_cpu_baseline:
+                    sys.path.insert(0, str(REPO / "oracle"))
+                    from grg_oracle import OracleGRG
+
+                    oracle = OracleGRG(path)
+                    oerr, perr = [], []
+                    for i in small:
+                        x_np = xs[i].cpu().numpy()
+                        m_np = misses[i].cpu().numpy() if misses[i] is not None else None
+                        ref = oracle.matmul(x_np, items[i][1], miss=m_np)
+                        oerr.append(rel(batch.outputs[i].cpu().numpy(), ref))
+                        perr.append(rel(plain_out[i], ref))
+                    out[name]["max_rel_err_vs_oracle_blocks_le3"] = max(oerr)
+                    out["plain_f64_dropin"]["max_rel_err_vs_oracle_blocks_le3"] = max(perr)
+            torch.cuda.empty_cache()
+    out["workload"] = (f"same graph; RHS blocks {blocks} in both directions (down with miss rows), "
+                       f"inputs copied into the op/batch buffers every step")
+    return out
 
 
 def run_reference(args) -> None:

@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -124,6 +124,8 @@ class TraverseArgs(ctypes.Structure):
         ("heavy_variant", ctypes.c_int32),
         ("mix_scratch", ctypes.c_void_p),
         ("mix_scratch_bytes", ctypes.c_int64),
+        ("narrow_split", ctypes.c_int32),
+        ("reserved2", ctypes.c_int32),
     ]
 
 

@@ -66,9 +66,13 @@ class B200Plan:
     is entered and use the fastest for this direction (instead of ``narrow_variant`` and
     ``heavy_variant``).
     ``pad_lists``: pad every gather list to a multiple of 4 entries (needed by variant 6).
-    ``heavy_variant``: heavy rows one warp each (1) or one CTA each (0); None picks per call
-    (warp for k <= 16, where a warp still splits a list over >= 4 lane groups; CTA above).
-    Exact order always uses CTAs.
+    ``heavy_variant``: heavy rows one CTA each (0), one warp each (1), or one warp each inside
+    the narrow-row launch (2, with ``narrow_variant`` 6); None picks per call (2 for k <= 16,
+    where a warp still splits a list over >= 4 lane groups, 0 above).  Exact order always
+    uses CTAs.
+    ``long_first``: with ``balance``, the longest length bucket is processed first.
+    ``narrow_split``: split each narrow row over 2^narrow_split lane groups (0..3; -1 chooses
+    per level; default mode with ``narrow_variant`` 6 only).
     """
 
     exact_order: bool = False
@@ -79,6 +83,8 @@ class B200Plan:
     autotune: bool = False
     pad_lists: bool = True
     heavy_variant: int | None = None
+    long_first: bool = True
+    narrow_split: int = 0
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -89,8 +95,10 @@ class B200Plan:
             raise ValueError(f"narrow_variant must be in [0, 7), got {self.narrow_variant}")
         if int(self.narrow_variant) == 6 and not self.pad_lists:
             raise ValueError("narrow_variant 6 reads padded gather lists; it needs pad_lists=True")
-        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1):
-            raise ValueError(f"heavy_variant must be 0 or 1, got {self.heavy_variant}")
+        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2):
+            raise ValueError(f"heavy_variant must be 0, 1 or 2, got {self.heavy_variant}")
+        if not -1 <= int(self.narrow_split) <= 3:
+            raise ValueError(f"narrow_split must be in [-1, 3], got {self.narrow_split}")
 
     def locality(self, direction: Direction) -> bool:
         if self.row_order is None:
@@ -100,7 +108,7 @@ class B200Plan:
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
-                   "heavy_variant"}
+                   "heavy_variant", "long_first", "narrow_split"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -108,7 +116,8 @@ class B200Plan:
                    heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)),
                    row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 6)),
                    balance=bool(value.get("balance", True)), autotune=bool(value.get("autotune", False)),
-                   pad_lists=bool(value.get("pad_lists", True)), heavy_variant=value.get("heavy_variant"))
+                   pad_lists=bool(value.get("pad_lists", True)), heavy_variant=value.get("heavy_variant"),
+                   long_first=bool(value.get("long_first", True)), narrow_split=int(value.get("narrow_split", 0)))
 
 
 @dataclass(frozen=True)
@@ -343,8 +352,8 @@ def plan_b200_layout(
 
     ``precision="plain"`` computes and stores in ``dtype``.  ``precision="mixed"`` (``dtype``
     must be float64: inputs and outputs stay FP64) keeps the node state in 6 bytes per value,
-    an FP32 value plus a 16-bit correction (relative rounding <= 2^-40 per node, integers below
-    2^40 exact), with FP64 accumulation; it needs padded lists and the default (not
+    an FP32 value plus a 16-bit correction (relative rounding <= 2^-39 per node, integers below
+    2^39 exact), with FP64 accumulation; it needs padded lists and the default (not
     exact-order) heavy-row mode."""
     dtype = np.dtype(dtype)
     if dtype not in (np.dtype(np.float32), np.dtype(np.float64)):

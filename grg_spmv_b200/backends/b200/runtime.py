@@ -288,14 +288,14 @@ class B200Runtime:
         if up_on:
             plan = lay.pair.plan_up
             built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance,
-                                                            plan.pad_lists)}
+                                                            plan.pad_lists, plan.long_first)}
             levels[Direction.UP] = self._upload_levels(art.levels_up, built)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
             plan = lay.pair.plan_down
             built = {lv.level: lv for lv in build_down_levels(
                 off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
-                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists)}
+                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first)}
             levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
         del coo
         return _DeviceArtifact(
@@ -383,7 +383,7 @@ class B200Runtime:
                 narrow_ms[variant] = timed()
             args.narrow_variant = min(narrow_ms, key=narrow_ms.get)
             heavy_ms = {}
-            for heavy in (0, 1):
+            for heavy in (0, 1, 2):
                 args.heavy_variant = heavy
                 heavy_ms[heavy] = timed()
         return int(args.narrow_variant), int(min(heavy_ms, key=heavy_ms.get))
@@ -484,7 +484,10 @@ class B200Runtime:
         a.error_word = _ptr(self._error_word) if self._check_bounds else None
         a.narrow_variant = int(self._variant.get(direction, plan.narrow_variant))
         heavy = self._heavy_variant.get(direction, plan.heavy_variant)
-        a.heavy_variant = int(heavy) if heavy is not None else (1 if k <= 16 else 0)
+        if heavy is None:  # as measured on B200: warps (fused into the narrow launch) for k <= 16
+            heavy = (2 if a.narrow_variant == 6 else 1) if k <= 16 else 0
+        a.heavy_variant = int(heavy)
+        a.narrow_split = int(plan.narrow_split)
         return a
 
     def _capturing(self) -> bool:

@@ -100,7 +100,7 @@ def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.nd
 
 def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
             group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True,
-            pad: bool = False) -> LevelGather:
+            pad: bool = False, long_first: bool = True) -> LevelGather:
     """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr.
 
     With ``locality`` the rows are stored in the order of the id of their last state entry
@@ -122,8 +122,9 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
     entries = (ids.astype(np.uint32) | (src.astype(np.uint32) << np.uint32(nat.SRC_SHIFT))
                | np.where(start, np.uint32(nat.SEG_START), np.uint32(0))).astype(np.uint32)
     # Processing order: narrow rows first, grouped into power-of-two length buckets so the rows
-    # of a warp need similar trip counts (in locality order inside a bucket when asked); heavy
-    # rows last.
+    # of a warp need similar trip counts (in locality order inside a bucket when asked), the
+    # longest bucket first (``long_first``: CTAs start in index order, so the longest chains of
+    # dependent loads start earliest and short rows fill in behind them); heavy rows last.
     perm = np.arange(num_rows, dtype=np.int64)
     if locality and num_rows > 1:
         key = np.full(num_rows, np.iinfo(np.int64).max, dtype=np.int64)
@@ -134,7 +135,7 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
         perm = np.argsort(key, kind="stable")
     if balance and num_rows > 1:
         bucket = np.ceil(np.log2(counts[perm] + 1.0)).astype(np.int64)
-        perm = perm[np.argsort(bucket, kind="stable")]
+        perm = perm[np.argsort(-bucket if long_first else bucket, kind="stable")]
     heavy_mask = counts[perm] > heavy_threshold
     perm = np.concatenate((perm[~heavy_mask], perm[heavy_mask]))
     num_heavy = int(heavy_mask.sum())
@@ -174,7 +175,7 @@ def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
 
 
 def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, locality: bool = False,
-                    balance: bool = True, pad: bool = False) -> list[LevelGather]:
+                    balance: bool = True, pad: bool = False, long_first: bool = True) -> list[LevelGather]:
     """Gather lists for up levels 1..h-1 (level 0 is seeded from the input)."""
     off = np.asarray(level_offsets, dtype=np.int64)
     h = off.size - 1
@@ -191,7 +192,7 @@ def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, 
             src.append(np.full(r.size, s, dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
-        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad))
+        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first))
     return levels
 
 
@@ -205,7 +206,8 @@ def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[
 
 
 def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int,
-                      locality: bool = True, balance: bool = True, pad: bool = False) -> list[LevelGather]:
+                      locality: bool = True, balance: bool = True, pad: bool = False,
+                      long_first: bool = True) -> list[LevelGather]:
     """Gather lists for down levels h-1..0 in execution order.
 
     ``sel_mut``/``sel_miss`` are (indptr, indices, num_mutations) triples; ``sel_miss`` may be
@@ -238,7 +240,7 @@ def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, h
             grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         levels.append(_finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
-                              cat(grp, np.int16), heavy_threshold, locality, balance, pad))
+                              cat(grp, np.int16), heavy_threshold, locality, balance, pad, long_first))
     return levels
 
 

@@ -156,6 +156,7 @@ struct LevelArgs {
     int64_t lim_state;
     int64_t lim_x;
     int64_t lim_miss;
+    int32_t log2s;  // narrow rows split over 2^log2s lane groups (default mode, variant 6)
     // mixed storage only: the 16-bit planes of state, x and miss (x/miss hold encoded copies)
     void* state_lo;
     const void* x_lo;
@@ -405,11 +406,11 @@ __global__ void __launch_bounds__(kAsyncThreads) level_async_kernel(LevelArgs a)
 // lane reads its row's codes four at a time with one aligned 16-byte load and loads the next
 // four while the current four rows are fetched, so each round waits on one memory latency.
 template <typename T, int V, int INIT>
-__global__ void __launch_bounds__(kNarrowThreads, 6) level_vec_kernel(LevelArgs a) {
+__device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
-    const int64_t pos = ((static_cast<int64_t>(blockIdx.x) * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
     if (pos >= narrow) return;  // no warp-wide operations below
     const int32_t e0 = __ldg(a.row_ptr + pos);
     const int32_t e1 = __ldg(a.row_ptr + pos + 1);
@@ -460,6 +461,64 @@ __device__ __forceinline__ Pack<T, V> shfl_xor_pack(const Pack<T, V>& x, int off
     return r;
 }
 
+// Narrow rows of padded lists, each split over 2^log2s lane groups (default mode only): group
+// j of a row takes quads j, j + 2^log2s, ... and the groups' sums are combined by an
+// xor-shuffle butterfly in a fixed order, so a row waits on ~1/2^log2s of the memory round
+// trips of vec_rows.  Used for levels whose rows are long but too few to fill the GPU.
+template <typename T, int V, int INIT>
+__device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int lg = a.log2g + a.log2s;  // lanes per row
+    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - lg)) + (lane >> lg);
+    const bool live = pos < narrow;  // dead lanes still join the shuffles
+    int32_t e0 = 0, e1 = 0;
+    int64_t row = 0;
+    if (live) {
+        e0 = __ldg(a.row_ptr + pos);
+        e1 = __ldg(a.row_ptr + pos + 1);
+        row = level_row(a, pos);
+    }
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int sub = (lane >> a.log2g) & ((1 << a.log2s) - 1);
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(glane) * V; c < a.k; c += step) {  // same trip count in every lane
+        Pack<T, V> part = zero_pack<T, V>();
+        if (live) {
+            for (int32_t q = (e0 >> 2) + sub; q < (e1 >> 2); q += 1 << a.log2s) {
+                const uint4 cq = __ldg(codes4 + q);
+                const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
+                Pack<T, V> val[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const T* src = entry_row<T>(a, code[u]);
+                    val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) add_into(part, val[u]);
+            }
+        }
+        for (int off = 1 << a.log2g; off < (1 << lg); off <<= 1) {
+            const Pack<T, V> other = shfl_xor_pack(part, off);
+            add_into(part, other);
+        }
+        if (live && sub == 0) {
+            Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+            add_into(acc, part);
+            st_pack(state + row * a.ld_state + c, acc);
+        }
+    }
+}
+
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kNarrowThreads, 6) level_vec_kernel(LevelArgs a) {
+    if (a.log2s > 0) split_rows<T, V, INIT>(a, blockIdx.x);
+    else vec_rows<T, V, INIT>(a, blockIdx.x);
+}
+
 constexpr int kWarpRowThreads = 256;
 
 // Heavy rows, one warp each (heavy_variant 1, default mode only).  Lane group g of 32/G
@@ -469,8 +528,8 @@ constexpr int kWarpRowThreads = 256;
 // integer data), and group 0 adds the init value and stores the row.  Compared with a CTA per
 // row this keeps eight heavy rows per CTA and needs no shared memory or block barriers.
 template <typename T, int V, int INIT>
-__global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a) {
-    const int64_t w = static_cast<int64_t>(blockIdx.x) * (kWarpRowThreads / 32) + (threadIdx.x >> 5);
+__device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t block) {
+    const int64_t w = block * (kWarpRowThreads / 32) + (threadIdx.x >> 5);
     if (w >= a.num_heavy) return;  // warp-uniform
     const int lane32 = threadIdx.x & 31;
     const int64_t pos = __ldg(a.heavy_rows + w);
@@ -529,15 +588,33 @@ __global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a
     }
 }
 
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a) {
+    warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
+}
+
+// One launch for a whole level (heavy_variant 2): the first ceil(num_heavy / 8) CTAs take the
+// heavy rows one warp each, so the longest lists start first, and the remaining CTAs take the
+// narrow rows as level_vec_kernel does.  The two kinds of rows are disjoint and read only
+// lower levels, so nothing orders them; this saves the second launch of a level and lets the
+// heavy rows overlap the narrow ones.
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kNarrowThreads, 6) level_fused_kernel(LevelArgs a, int64_t heavy_blocks) {
+    static_assert(kNarrowThreads == kWarpRowThreads, "both row kinds use the same CTA shape");
+    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
+    else if (a.log2s > 0) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+    else vec_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+}
+
 // ---------------------------------------------------------------------------------------
 // Mixed storage (dtype GRG_B200_MIXED)
 //
-// A value v is stored in 6 bytes as hi = v rounded to FP32 plus a 16-bit signed correction
-// lo, so that v ~= hi + lo * 2^(e(hi) - 39), where e(hi) is hi's unbiased exponent (FP32
-// subnormals use the smallest normal exponent).  hi carries 24 significant bits and lo 16
-// more, so a stored value is within 2^-40 of v relative to |hi| and integers below 2^40 are
-// exact.  Decoding is exact in FP64 (24 + 16 bits fit in 53), every sum is accumulated in
-// FP64 registers and rounded back to 6 bytes once per node.  A buffer of R rows and ld
+// A value v is stored in 6 bytes as hi = v rounded to nearest FP32 plus a 16-bit signed
+// correction lo, so that v ~= hi + lo * 2^(e(hi) - 38), where e(hi) is hi's unbiased exponent
+// (FP32 subnormals use the smallest normal exponent).  |v - hi| is at most half an FP32 ulp,
+// 2^(e - 24), so |lo| <= 2^14 always fits; the stored value is within 2^-39 of v relative to
+// |hi| and integers below 2^39 are exact.  Decoding is exact in FP64 (24 + 15 bits fit in 53),
+// every sum is accumulated in FP64 registers and rounded back to 6 bytes once per node.  A buffer of R rows and ld
 // columns (ld % 4 == 0) is two planes: float hi[R * ld] followed by int16 lo[R * ld].
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t mx_exp_field(float hi) {
@@ -545,13 +622,13 @@ __device__ __forceinline__ uint32_t mx_exp_field(float hi) {
     return e == 0u ? 1u : e;
 }
 
-// 2^(e - 39) for the biased exponent field E = e + 127: 2^(E - 166) as a double.
+// 2^(e - 38) for the biased exponent field E = e + 127: 2^(E - 165) as a double.
 __device__ __forceinline__ double mx_unit(float hi) {
-    return __longlong_as_double(static_cast<long long>(mx_exp_field(hi) + (1023u - 166u)) << 52);
+    return __longlong_as_double(static_cast<long long>(mx_exp_field(hi) + (1023u - 165u)) << 52);
 }
 
 __device__ __forceinline__ double mx_inv_unit(float hi) {
-    return __longlong_as_double(static_cast<long long>((1023u + 166u) - mx_exp_field(hi)) << 52);
+    return __longlong_as_double(static_cast<long long>((1023u + 165u) - mx_exp_field(hi)) << 52);
 }
 
 __device__ __forceinline__ double mx_decode(float hi, short lo) {
@@ -565,9 +642,7 @@ __device__ __forceinline__ void mx_encode(double v, float& hi, short& lo) {
         return;
     }
     const double r = v - static_cast<double>(hi);  // exact
-    int q = __double2int_rn(r * mx_inv_unit(hi));    // |q| <= 2^15
-    q = q > 32767 ? 32767 : (q < -32768 ? -32768 : q);
-    lo = static_cast<short>(q);
+    lo = static_cast<short>(__double2int_rn(r * mx_inv_unit(hi)));  // |lo| <= 2^14
 }
 
 struct Quad {
@@ -1173,7 +1248,8 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
     if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
-    if (a->heavy_variant < 0 || a->heavy_variant > 1) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 1]", a->heavy_variant);
+    if (a->heavy_variant < 0 || a->heavy_variant > 2) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 2]", a->heavy_variant);
+    if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
     if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
     if (a->init_mode == GRG_B200_INIT_XTX && !a->xtx_node) return fail(GRG_B200_ERR_INVALID, "xtx_node is NULL");
     if (a->init_mode == GRG_B200_INIT_MATRIX && (!a->init_matrix || !a->node_perm || a->ld_init < a->k))
@@ -1224,8 +1300,24 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
 template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
+    if (variant == 6 && heavy_variant == 2 && !exact) {
+        constexpr int rows_per_cta = kWarpRowThreads / 32;
+        const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
+        const int lg = la.log2g + la.log2s;
+        const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
+        const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
+        switch (init_mode) {
+            case 0: level_fused_kernel<T, V, 0><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
+            case 1: level_fused_kernel<T, V, 1><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
+            case 2: level_fused_kernel<T, V, 2><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
+            default: level_fused_kernel<T, V, 3><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
+        }
+        GRG_LAUNCH_CHECK("level_fused_kernel");
+        return GRG_B200_OK;
+    }
     if (narrow > 0 && variant == 6) {
-        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        const int lg = la.log2g + la.log2s;
+        const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
         switch (init_mode) {
             case 0: level_vec_kernel<T, V, 0><<<grid, kNarrowThreads, 0, s>>>(la); break;
@@ -1266,7 +1358,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
 #undef GRG_NARROW
         GRG_LAUNCH_CHECK("level_narrow_kernel");
     }
-    if (la.num_heavy > 0 && !exact && heavy_variant == 1) {
+    if (la.num_heavy > 0 && !exact && heavy_variant >= 1) {
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
         switch (init_mode) {
@@ -1353,6 +1445,20 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     if (L->list_align == 4 && (L->off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
     la.list_align = L->list_align;
     la.num_heavy = L->num_heavy;
+    la.log2s = 0;
+    if (a->exact_order == 0 && a->narrow_variant == 6 && a->dtype != GRG_B200_MIXED) {
+        if (a->narrow_split >= 0) {
+            la.log2s = a->narrow_split;
+        } else {  // split long rows while the level alone would not fill the GPU twice over
+            const int64_t narrow_rows = L->num_rows - L->num_heavy;
+            const int64_t quads = narrow_rows > 0 ? (L->num_entries / 4) / narrow_rows : 0;
+            const int64_t target_warps = 148 * 48 * 2;
+            while (la.log2s < 3 && sh.log2g + la.log2s < 5 && (int64_t{2} << la.log2s) <= quads &&
+                   ((narrow_rows << (sh.log2g + la.log2s + 1)) >> 5) <= target_warps)
+                ++la.log2s;
+        }
+        if (sh.log2g + la.log2s > 5) la.log2s = 5 - sh.log2g;
+    }
     la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
     const bool exact = a->exact_order != 0;
     if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, s);

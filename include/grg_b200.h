@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 6
+#define GRG_B200_ABI_VERSION 7
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -67,8 +67,8 @@ typedef enum grg_b200_status {
 /*
  * GRG_B200_MIXED: input, output, miss and init buffers are FP64; the node state (and, for
  * down, encoded copies of input and miss in mix_scratch) is stored in 6 bytes per value:
- * hi = the value rounded to FP32 and lo = a 16-bit correction in units of 2^(e(hi) - 39), so
- * a stored value is within 2^-40 of the exact one relative to |hi| (integers below 2^40 are
+ * hi = the value rounded to FP32 and lo = a 16-bit correction in units of 2^(e(hi) - 38), so
+ * a stored value is within 2^-39 of the exact one relative to |hi| (integers below 2^39 are
  * exact).  Sums are accumulated in FP64 and rounded back once per node.  A mixed buffer of
  * R rows and ld columns (ld a multiple of 4) is float hi[R * ld] followed by int16
  * lo[R * ld]; see GRG_B200_MIX_BYTES.  Mixed traversals never use exact order.
@@ -193,11 +193,17 @@ typedef struct grg_b200_traverse_args {
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
-                                           reduction).  Exact order always uses one CTA per row. */
+                                           reduction); 2 as 1 but in the same launch as the narrow
+                                           rows (narrow_variant 6 only; otherwise as 1).  Exact
+                                           order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of
                                            num_mutations rows and ld_state columns */
     int64_t mix_scratch_bytes;
+    int32_t narrow_split;               /* narrow_variant 6, default mode, FP64/FP32: split each narrow
+                                           row over 2^narrow_split lane groups (0..3), or -1 to choose
+                                           per level (long rows in levels too small to fill the GPU) */
+    int32_t reserved2;
 } grg_b200_traverse_args;
 
 #define GRG_B200_NARROW_VARIANTS 7

@@ -82,7 +82,7 @@ def test_mixed_against_oracle(synth_artifact, k, heavy):
 
 
 def test_mixed_large_integers_stay_exact(synth_artifact):
-    """Integer inputs whose node sums reach ~2^33 are still exact (stored values carry 40 bits)."""
+    """Integer inputs whose node sums reach ~2^33 are still exact (stored values carry 39 bits)."""
     oracle = OracleGRG(synth_artifact)
     rng = np.random.default_rng(7)
     with _runtime(synth_artifact, 4) as runtime:

@@ -75,15 +75,17 @@ def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
         assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("heavy_variant", [0, 1])
+@pytest.mark.parametrize("heavy_variant", [0, 1, 2])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_fast_mode_heavy_rows(group, heavy_variant, golden_data):
-    """Default mode with split heavy rows (one CTA or one warp per row, fixed-order
-    reductions): exact for integer-valued inputs, tolerance otherwise."""
+    """Default mode with split heavy rows (one CTA or one warp per row, the warps also fused
+    into the narrow launch; fixed-order reductions): exact for integer-valued inputs,
+    tolerance otherwise."""
     from grg_spmv_b200.backends.b200 import B200Runtime
 
     name, dtype = group
-    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=False, heavy=2, heavy_variant=heavy_variant)
+    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), exact=False, heavy=2, heavy_variant=heavy_variant,
+                     variant=6 if heavy_variant == 2 else 0)
     rtol, atol = (RTOL_F64, ATOL_F64) if dtype == "float64" else (RTOL_F32, ATOL_F32)
     with B200Runtime(layout, check_bounds=True) as runtime:
         (grg,) = runtime.grgs

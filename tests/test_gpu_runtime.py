@@ -106,12 +106,12 @@ def test_up_output_aliases_down_input():
 def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     """Integer-valued inputs are exact; real-valued inputs agree to 1e-12 (default heavy-row
     reduction) — every mode of the hot path on a 60k-node graph with random node ids.  Heavy
-    rows go to the CTA-per-row kernel with narrow variants 0/4 and to the warp-per-row kernel
-    with 5/6, so every k runs both."""
+    rows go to the CTA-per-row kernel with narrow variants 0/4, to the warp-per-row kernel with
+    5 and to the fused narrow+heavy launch with 6, so every k runs all three."""
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
 
     oracle = OracleGRG(synth_artifact)
-    heavy_variant = 1 if variant in (5, 6) else 0
+    heavy_variant = {5: 1, 6: 2}.get(variant, 0)
     pair = B200PlanPair(plan_up=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant),
                         plan_down=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant))
     rng = np.random.default_rng(100 + k)
@@ -345,7 +345,7 @@ def test_autotune_picks_a_known_variant_and_stays_exact(synth_artifact):
     with _runtime(_layout([synth_artifact], requirements=_req(k=4), pair=pair)) as runtime:
         assert set(runtime._variant) == {"up", "down"} == set(runtime._heavy_variant)
         assert all(v in B200Runtime.TUNE_VARIANTS for v in runtime._variant.values())
-        assert all(v in (0, 1) for v in runtime._heavy_variant.values())
+        assert all(v in (0, 1, 2) for v in runtime._heavy_variant.values())
         (grg,) = runtime.grgs
         for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
             x = _pm1(rng, (4, cols))
