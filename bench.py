@@ -71,6 +71,8 @@ def parse_args():
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
     p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
+    p.add_argument("--schedule", choices=["levels", "dataflow"], default=None,
+                   help="one launch per level, or one persistent dataflow launch per traversal")
     p.add_argument("--precision", choices=["plain", "mixed"], default="plain",
                    help="node state in FP64 (plain) or FP32 + 16-bit correction with FP64 sums (mixed)")
     p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
@@ -222,6 +224,8 @@ def run_b200(args) -> None:
         extra["long_first"] = False
     if args.narrow_split is not None:
         extra["narrow_split"] = args.narrow_split
+    if args.schedule is not None:
+        extra["schedule"] = args.schedule
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
                         plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
     stream = torch.cuda.Stream(device=device)
@@ -302,6 +306,16 @@ def run_b200(args) -> None:
         torch.cuda._sleep(100_000_000)
         for name, op in (("up", up), ("down", down)):
             args_c = op._args
+            if pair.plan_down.schedule == "dataflow":  # one persistent launch per traversal: time the whole call
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                nat.check(lib, lib.grg_b200_traverse(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "traverse")
+                b.record(stream)
+                level_launches += 3 if name == "up" else 2  # sentinel fill (+ seed) + dataflow kernel + output
+                lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
+                units = [level_units(scan, name, L, True) for L in lv_order if scan.level_sizes[L] > 0]
+                all_evs.append((name, [(a, b)], [], units))
+                continue
             if name == "up":
                 nat.check(lib, lib.grg_b200_seed_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "seed_up")
             levels = runtime._artifacts[0].levels[op._spec.direction]
@@ -313,7 +327,7 @@ def run_b200(args) -> None:
                                                       ctypes.c_void_p(stream.cuda_stream)), "run_level")
                 b.record(stream)
                 evs.append((a, b))
-                fused = op._args.heavy_variant == 2 and op._args.narrow_variant == 6 and not op._args.exact_order
+                fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                 level_launches += 1 + (1 if levels.array[i].num_heavy > 0 and not fused else 0)
             if name == "up":
                 nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
@@ -325,13 +339,15 @@ def run_b200(args) -> None:
         torch.cuda.synchronize(device)
         for name, evs, lvs, units in all_evs:
             level_ms[name] = sum(a.elapsed_time(b) for a, b in evs)
+            if not lvs:
+                print(f"[traversal] {name} entries={sum(u[1] for u in units)} ms={level_ms[name]:.4f}", file=sys.stderr)
             for (a, b), lv, unit in zip(evs, lvs, units):
                 ms = a.elapsed_time(b)
                 nbytes = level_bytes([unit], k, vb, "up", M, False)
                 print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
             lv_bytes += level_bytes(units, k, vb, name, M, use_miss=True)
-    launches_per_step = level_launches + 1 + 1 + 1  # + seed_up + output_up + output_down
+    launches_per_step = level_launches + (0 if pair.plan_down.schedule == "dataflow" else 3)  # + seed_up + outputs
     level_total_ms = level_ms["up"] + level_ms["down"]
     peak, peak_kind = measured_peak_hbm()
     achieved = lv_bytes / (level_total_ms / 1e3) / 1e9
@@ -395,6 +411,7 @@ def run_b200(args) -> None:
 
     tuned = {d.value: [v, runtime._heavy_variant.get(d)] for d, v in runtime._variant.items()}
     heavy_used = {"up": int(up._args.heavy_variant), "down": int(down._args.heavy_variant)}
+    narrow_used = {"up": int(up._args.narrow_variant), "down": int(down._args.narrow_variant)}
     runtime.__exit__(None, None, None)
     del up, down, runtime
     torch.cuda.empty_cache()
@@ -419,15 +436,18 @@ def run_b200(args) -> None:
                                    f"1% missing, fully resident, up+down per step",
                        "k": k, "precision": args.precision, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
-                       "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": pair.plan_down.narrow_variant,
+                       "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
                        "long_first": pair.plan_down.long_first, "narrow_split": pair.plan_down.narrow_split,
+                       "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
                        "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "level gathers (narrow-row kernel of the plan + heavy-row kernel)",
+                         "traffic": None, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
+                                    if pair.plan_down.schedule == "dataflow" else
+                                    "level gathers (one fused narrow+heavy launch per level)"),
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
                          "level_ms_per_step": level_total_ms, "level_bytes_per_step": lv_bytes},
             "cpu_baseline": cpu,

@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -28,6 +28,8 @@ NVCC_FLAGS = (
 # Status codes, enums and entry coding (grg_b200.h).
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED = 0, 1, 2, 3
 F64, F32, MIXED = 0, 1, 2
+SCHEDULE_LEVELS, SCHEDULE_DATAFLOW = 0, 1
+DEVICE_WAIT_TIMEOUT = 6
 UP, DOWN = 0, 1
 INIT_NONE, INIT_VECTOR, INIT_XTX, INIT_MATRIX = 0, 1, 2, 3
 BIAS_NONE, BIAS_VECTOR, BIAS_XTX = 0, 1, 2
@@ -53,7 +55,7 @@ SRC_SHIFT = 29
 SRC_STATE, SRC_INPUT, SRC_MISS, SRC_NULL = 0, 1, 2, 3
 ID_MASK = 0x1FFFFFFF
 MAX_ID = 0x1FFFFFFF
-NARROW_VARIANTS = 7
+NARROW_VARIANTS = 8
 
 
 class Level(ctypes.Structure):
@@ -125,7 +127,8 @@ class TraverseArgs(ctypes.Structure):
         ("mix_scratch", ctypes.c_void_p),
         ("mix_scratch_bytes", ctypes.c_int64),
         ("narrow_split", ctypes.c_int32),
-        ("reserved2", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("dataflow_sync", ctypes.c_void_p),
     ]
 
 

@@ -51,6 +51,7 @@ class _Tile:
     state: object
     scratch: object
     stream: object
+    sync: object
 
 
 @dataclass
@@ -174,12 +175,13 @@ class B200BatchedMatmul:
                                       init_mode=InitMode.NONE, backend_init_mode=InitMode.NONE, use_miss=g.use_miss,
                                       input_cols=g.io_in.shape[0], output_cols=g.io_out.shape[0], apply_endpoint_bias=False)
                 miss_view = g.miss_in[:, c0:c0 + w] if g.use_miss else None
+                sync = torch.zeros(4, device=rt.device, dtype=torch.int32)  # own dataflow counter per tile
                 args = rt._traverse_args(art, spec, g.io_in[:, c0:c0 + w], g.io_out[:, c0:c0 + w], miss_view, None, None,
-                                         state=state, mixed=mixed, mix_scratch=scratch)
+                                         state=state, mixed=mixed, mix_scratch=scratch, df_sync=sync)
                 args.ring = None  # resident levels only (checked when the groups were built)
                 stream = torch.cuda.Stream(device=rt.device)
                 streams.append(stream)
-                g.tiles.append(_Tile(args=args, state=state, scratch=scratch, stream=stream))
+                g.tiles.append(_Tile(args=args, state=state, scratch=scratch, stream=stream, sync=sync))
                 c0 += w
         self._graph = self._capture() if rt._use_graphs else None
 

@@ -59,7 +59,9 @@ class B200Plan:
     ``heavy_threshold``: rows with more entries than this go to the heavy-row kernel.
     ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
     processed together); None picks the direction's default (up natural, down locality).
-    ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``).
+    ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``); None
+    picks per call from the padded-list kernels (7 for k <= 16, 6 above, as measured on
+    B200; with ``pad_lists=False``, 5).
     ``balance``: group narrow rows by length (power-of-two buckets) so a warp's rows finish
     together.
     ``autotune``: time the narrow-kernel variants, then the heavy-row kernels, when the runtime
@@ -67,38 +69,51 @@ class B200Plan:
     ``heavy_variant``).
     ``pad_lists``: pad every gather list to a multiple of 4 entries (needed by variant 6).
     ``heavy_variant``: heavy rows one CTA each (0), one warp each (1), or one warp each inside
-    the narrow-row launch (2, with ``narrow_variant`` 6); None picks per call (2 for k <= 16,
-    where a warp still splits a list over >= 4 lane groups, 0 above).  Exact order always
-    uses CTAs.
+    the narrow-row launch (2, with ``narrow_variant`` 6 or 7); None picks 2 with the padded
+    variants and otherwise 1 for k <= 16, 0 above.  Exact order always uses CTAs.
     ``long_first``: with ``balance``, the longest length bucket is processed first.
     ``narrow_split``: split each narrow row over 2^narrow_split lane groups (0..3; -1 chooses
-    per level; default mode with ``narrow_variant`` 6 only).
+    per level; default mode with ``narrow_variant`` 6 or 7 only).
+    ``schedule``: "levels" (one launch per level) or "dataflow" (one persistent launch per
+    traversal, rows wait only for their own sources; default mode, resident levels, padded
+    lists, plain precision; other calls fall back to "levels").
     """
 
     exact_order: bool = False
     heavy_threshold: int = DEFAULT_HEAVY_THRESHOLD
     row_order: str | None = None
-    narrow_variant: int = 6
+    narrow_variant: int | None = None
     balance: bool = True
     autotune: bool = False
     pad_lists: bool = True
     heavy_variant: int | None = None
     long_first: bool = True
-    narrow_split: int = 0
+    narrow_split: int = -1
+    schedule: str = "levels"
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
         if self.row_order not in (None, "natural", "locality"):
             raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
-        if not 0 <= int(self.narrow_variant) < 7:
-            raise ValueError(f"narrow_variant must be in [0, 7), got {self.narrow_variant}")
-        if int(self.narrow_variant) == 6 and not self.pad_lists:
-            raise ValueError("narrow_variant 6 reads padded gather lists; it needs pad_lists=True")
+        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < 8:
+            raise ValueError(f"narrow_variant must be in [0, 8), got {self.narrow_variant}")
+        if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
+            raise ValueError("narrow_variants 6 and 7 read padded gather lists; they need pad_lists=True")
         if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2):
             raise ValueError(f"heavy_variant must be 0, 1 or 2, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:
             raise ValueError(f"narrow_split must be in [-1, 3], got {self.narrow_split}")
+        if self.schedule not in ("levels", "dataflow"):
+            raise ValueError(f"schedule must be 'levels' or 'dataflow', got {self.schedule!r}")
+
+    def resolve_narrow_variant(self, k: int) -> int:
+        """The narrow-row kernel variant used for a call with ``k`` right-hand sides."""
+        if self.narrow_variant is not None:
+            return int(self.narrow_variant)
+        if not self.pad_lists:
+            return 5
+        return 7 if int(k) <= 16 else 6
 
     def locality(self, direction: Direction) -> bool:
         if self.row_order is None:
@@ -108,16 +123,17 @@ class B200Plan:
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
-                   "heavy_variant", "long_first", "narrow_split"}
+                   "heavy_variant", "long_first", "narrow_split", "schedule"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
         return cls(exact_order=bool(value.get("exact_order", False)),
                    heavy_threshold=int(value.get("heavy_threshold", DEFAULT_HEAVY_THRESHOLD)),
-                   row_order=value.get("row_order"), narrow_variant=int(value.get("narrow_variant", 6)),
+                   row_order=value.get("row_order"), narrow_variant=value.get("narrow_variant"),
                    balance=bool(value.get("balance", True)), autotune=bool(value.get("autotune", False)),
                    pad_lists=bool(value.get("pad_lists", True)), heavy_variant=value.get("heavy_variant"),
-                   long_first=bool(value.get("long_first", True)), narrow_split=int(value.get("narrow_split", 0)))
+                   long_first=bool(value.get("long_first", True)), narrow_split=int(value.get("narrow_split", -1)),
+                   schedule=str(value.get("schedule", "levels")))
 
 
 @dataclass(frozen=True)

@@ -160,6 +160,7 @@ class B200Runtime:
         self._io1 = None
         self._aux = None
         self._error_word = None
+        self._df_sync = None
         self._slots = []
         self._slot_ptrs = None
         self._slot_bytes = None
@@ -214,6 +215,7 @@ class B200Runtime:
                 self._io1 = None if io1_rows == 0 else torch.zeros((io1_rows, max_k), device=self.device, dtype=tdt)
                 self._aux = torch.zeros((lay.max_num_nodes, max_k), device=self.device, dtype=tdt)
                 self._error_word = torch.zeros(64, device=self.device, dtype=torch.int32)
+                self._df_sync = torch.zeros(4, device=self.device, dtype=torch.int32)  # dataflow task counter/flags
                 self._slots = [torch.empty(int(n), device=self.device, dtype=torch.uint8) for n in lay.slot_bytes]
                 if self._slots:
                     self._slot_ptrs = (ctypes.c_void_p * len(self._slots))(*[s.data_ptr() for s in self._slots])
@@ -341,7 +343,7 @@ class B200Runtime:
         return _DeviceLevels(array=arr, keepalive=keep)
 
     # -- autotuning ------------------------------------------------------------------------------
-    TUNE_VARIANTS = (5, 6, 0, 1, 4)
+    TUNE_VARIANTS = (5, 6, 7, 0, 1, 4)
 
     def _tune_direction(self, direction: Direction) -> tuple[int, int]:
         """Fastest (narrow variant, heavy variant) for ``direction`` on the first artifact at
@@ -377,7 +379,7 @@ class B200Runtime:
         with torch.cuda.device(self.device), torch.cuda.stream(self._caller_stream):
             narrow_ms = {}
             for variant in self.TUNE_VARIANTS:
-                if variant == 6 and not plan.pad_lists:
+                if variant >= 6 and not plan.pad_lists:
                     continue
                 args.narrow_variant = variant
                 narrow_ms[variant] = timed()
@@ -412,7 +414,7 @@ class B200Runtime:
         return B200PreparedMatmul(self, self._artifacts[int(grg._artifact_index)], spec)
 
     def _traverse_args(self, art: _DeviceArtifact, spec, input_view, output_view, miss_view, init_vector, init_matrix, *,
-                       state=None, mixed: bool | None = None, mix_scratch=None):
+                       state=None, mixed: bool | None = None, mix_scratch=None, df_sync=None):
         st = art.state
         k = int(spec.k)
         direction = Direction(spec.direction)
@@ -482,12 +484,14 @@ class B200Runtime:
             a.slot_bytes = ctypes.cast(self._slot_bytes, ctypes.POINTER(ctypes.c_int64))
             a.num_slots = len(self._slots)
         a.error_word = _ptr(self._error_word) if self._check_bounds else None
-        a.narrow_variant = int(self._variant.get(direction, plan.narrow_variant))
+        a.narrow_variant = int(self._variant.get(direction, plan.resolve_narrow_variant(k)))
         heavy = self._heavy_variant.get(direction, plan.heavy_variant)
-        if heavy is None:  # as measured on B200: warps (fused into the narrow launch) for k <= 16
-            heavy = (2 if a.narrow_variant == 6 else 1) if k <= 16 else 0
+        if heavy is None:  # as measured on B200: warps fused into the narrow launch (k = 1, 8, 32)
+            heavy = 2 if a.narrow_variant >= 6 else (1 if k <= 16 else 0)
         a.heavy_variant = int(heavy)
         a.narrow_split = int(plan.narrow_split)
+        a.schedule = nat.SCHEDULE_DATAFLOW if plan.schedule == "dataflow" else nat.SCHEDULE_LEVELS
+        a.dataflow_sync = _ptr(self._df_sync if df_sync is None else df_sync)
         return a
 
     def _capturing(self) -> bool:
@@ -537,9 +541,10 @@ class B200Runtime:
         return B200BatchedMatmul(self, items, precision=precision, tile_k=tile_k, autotune=autotune)
 
     def device_error(self) -> int:
-        """Synchronise the caller stream and return the first failed device bounds check (0 = none)."""
+        """Synchronise the caller stream and return the first device error code (0 = none): a
+        failed bounds check, or a dataflow wait that timed out."""
         self._caller_stream.synchronize()
-        return int(self._error_word[0].item())
+        return int(self._error_word[0].item()) or int(self._df_sync[2].item())
 
 
 __all__ = ["B200PreparedMatmul", "B200Runtime"]

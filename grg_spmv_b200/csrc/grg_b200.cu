@@ -169,6 +169,7 @@ enum DeviceError : int32_t {
     kErrMissId = 3,
     kErrPerm = 4,
     kErrSelector = 5,
+    kErrWaitTimeout = 6,  // dataflow: a source row never became ready within the spin limit
 };
 
 __device__ __forceinline__ void report(int32_t* err, int32_t code) {
@@ -513,10 +514,11 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
     }
 }
 
-template <typename T, int V, int INIT>
-__global__ void __launch_bounds__(kNarrowThreads, 6) level_vec_kernel(LevelArgs a) {
-    if (a.log2s > 0) split_rows<T, V, INIT>(a, blockIdx.x);
-    else vec_rows<T, V, INIT>(a, blockIdx.x);
+// MB = CTAs per SM the register budget is sized for: 6 (narrow_variant 6, 40 registers) or 5
+// (narrow_variant 7, 48 registers: no spills, fewer warps).
+template <typename T, int V, int INIT, int MB>
+__global__ void __launch_bounds__(kNarrowThreads, MB) level_vec_kernel(LevelArgs a) {
+    vec_rows<T, V, INIT>(a, blockIdx.x);
 }
 
 constexpr int kWarpRowThreads = 256;
@@ -598,11 +600,11 @@ __global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a
 // narrow rows as level_vec_kernel does.  The two kinds of rows are disjoint and read only
 // lower levels, so nothing orders them; this saves the second launch of a level and lets the
 // heavy rows overlap the narrow ones.
-template <typename T, int V, int INIT>
-__global__ void __launch_bounds__(kNarrowThreads, 6) level_fused_kernel(LevelArgs a, int64_t heavy_blocks) {
+template <typename T, int V, int INIT, bool SPLIT, int MB>
+__global__ void __launch_bounds__(kNarrowThreads, MB) level_fused_kernel(LevelArgs a, int64_t heavy_blocks) {
     static_assert(kNarrowThreads == kWarpRowThreads, "both row kinds use the same CTA shape");
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
-    else if (a.log2s > 0) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+    else if constexpr (SPLIT) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
     else vec_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
 }
 
@@ -990,6 +992,242 @@ __global__ void __launch_bounds__(kWideThreads) level_wide_kernel(LevelArgs a) {
     }
 }
 
+// ---------------------------------------------------------------------------------------
+// Dataflow traversal (schedule GRG_B200_SCHEDULE_DATAFLOW): one persistent launch walks every
+// level.  Warps take tasks (a heavy row, or the narrow rows of one warp) from a global
+// counter in execution order, so every source of a task belongs to an earlier task that a
+// running warp already holds; a row therefore waits only for its own sources, not for the
+// whole previous level.  Readiness travels with the data: before the launch the rows this
+// traversal writes are filled with a NaN sentinel, and a reader re-loads (from L2) any value
+// that still holds it.  Every wait is bounded: after kSpinLimit retries the warp records
+// kErrWaitTimeout, raises the abort flag (which every warp polls) and stops.
+// ---------------------------------------------------------------------------------------
+constexpr int kDfMaxLevels = 128;
+constexpr int kDfThreads = 256;
+constexpr int kDfGrab = 2;          // tasks taken per counter increment
+constexpr int kSpinLimit = 1 << 20;  // retries of one load (each after a ~100 ns sleep)
+
+struct DfLevel {
+    const int32_t* row_ptr;
+    const uint4* codes;
+    const int32_t* row_ids;
+    int64_t row_begin;
+    int32_t num_rows;
+    int32_t num_heavy;
+};
+
+struct DfArgs {
+    LevelArgs a;          // shared fields: state, inputs, init, k, log2g, limits, error word
+    int32_t* sync;        // [0] task counter, [1] abort flag, [2] status (zeroed before the launch)
+    int32_t total_tasks;
+    int32_t num_levels;
+    int32_t task_begin[kDfMaxLevels + 1];
+    DfLevel lv[kDfMaxLevels];
+};
+
+template <typename T>
+struct SentinelBits;
+template <>
+struct SentinelBits<double> {
+    static constexpr unsigned long long value = 0xFFF80DEADBEEF001ull;  // a quiet NaN no sum produces from finite data
+};
+template <>
+struct SentinelBits<float> {
+    static constexpr unsigned value = 0xFFC0DEADu;
+};
+
+__device__ __forceinline__ bool is_sentinel(double x) {
+    return static_cast<unsigned long long>(__double_as_longlong(x)) == SentinelBits<double>::value;
+}
+__device__ __forceinline__ bool is_sentinel(float x) { return __float_as_uint(x) == SentinelBits<float>::value; }
+
+template <typename T, int V>
+__device__ __forceinline__ bool any_sentinel(const Pack<T, V>& p) {
+    bool s = false;
+#pragma unroll
+    for (int i = 0; i < V; ++i) s |= is_sentinel(p.v[i]);
+    return s;
+}
+
+// L2 load (rows written by other SMs during this launch must not come from a stale L1 line).
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> ld_l2(const T* p) {
+    Pack<T, V> r;
+    if constexpr (V == 1) {
+        r.v[0] = __ldcg(p);
+    } else if constexpr (std::is_same<T, double>::value && V == 2) {
+        const double2 d = __ldcg(reinterpret_cast<const double2*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else if constexpr (std::is_same<T, float>::value && V == 2) {
+        const float2 d = __ldcg(reinterpret_cast<const float2*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else {
+        const float4 d = __ldcg(reinterpret_cast<const float4*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+        r.v[2] = d.z;
+        r.v[3] = d.w;
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool df_aborted(const DfArgs& p) {
+    return *reinterpret_cast<volatile const int32_t*>(p.sync + 1) != 0;
+}
+
+// Re-load a state row until it no longer holds the sentinel (bounded).
+template <typename T, int V>
+__device__ __noinline__ Pack<T, V> df_wait(const DfArgs& p, const T* src, Pack<T, V> v) {
+    for (int spin = 0; any_sentinel(v); ++spin) {
+        if (spin >= kSpinLimit || df_aborted(p)) {
+            if (spin >= kSpinLimit) {
+                report(p.a.err, kErrWaitTimeout);
+                atomicCAS(p.sync + 2, 0, kErrWaitTimeout);
+            }
+            atomicExch(p.sync + 1, 1);
+            return zero_pack<T, V>();
+        }
+        __nanosleep(100);
+        v = ld_l2<T, V>(src);
+    }
+    return v;
+}
+
+// Fetch one entry's row: state rows through L2 with the readiness check, inputs as usual.
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> df_fetch(const DfArgs& p, uint32_t code, int64_t c) {
+    const uint32_t src = (code >> GRG_B200_SRC_SHIFT) & GRG_B200_SRC_MASK;
+    if (src == GRG_B200_SRC_STATE) {
+        const T* row = entry_row<T>(p.a, code);
+        if (!row) return zero_pack<T, V>();
+        Pack<T, V> v = ld_l2<T, V>(row + c);
+        if (any_sentinel(v)) v = df_wait<T, V>(p, row + c, v);
+        return v;
+    }
+    const T* row = entry_row<T>(p.a, code);
+    return row ? ld_ro<T, V>(row + c) : zero_pack<T, V>();
+}
+
+template <typename T, int V, int INIT>
+__device__ __forceinline__ void df_narrow(const DfArgs& p, const DfLevel& L, int64_t task) {
+    const LevelArgs& a = p.a;
+    const int lane = threadIdx.x & 31;
+    const int64_t narrow = L.num_rows - L.num_heavy;
+    const int64_t pos = (task << (5 - a.log2g)) + (lane >> a.log2g);
+    if (pos >= narrow) return;
+    const int32_t e0 = __ldg(L.row_ptr + pos);
+    const int32_t e1 = __ldg(L.row_ptr + pos + 1);
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int64_t row = L.row_begin + (L.row_ids ? static_cast<int64_t>(__ldg(L.row_ids + pos)) : pos);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(glane) * V; c < a.k; c += step) {
+        Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+        Pack<T, V> seg = zero_pack<T, V>();
+        const int32_t q1 = e1 >> 2;
+        int32_t q = e0 >> 2;
+        uint4 cur = q < q1 ? __ldg(L.codes + q) : null4;
+        for (; q < q1; ++q) {
+            const uint4 nxt = q + 1 < q1 ? __ldg(L.codes + q + 1) : null4;
+            const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+            Pack<T, V> val[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) val[u] = df_fetch<T, V>(p, code[u], c);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (code[u] & GRG_B200_SEG_START) {
+                    add_into(acc, seg);
+                    seg = zero_pack<T, V>();
+                }
+                add_into(seg, val[u]);  // skipped entries fetch +0
+            }
+            cur = nxt;
+        }
+        add_into(acc, seg);
+        st_pack(state + row * a.ld_state + c, acc);
+    }
+}
+
+template <typename T, int V, int INIT>
+__device__ __forceinline__ void df_heavy(const DfArgs& p, const DfLevel& L, int64_t h) {
+    const LevelArgs& a = p.a;
+    const int lane32 = threadIdx.x & 31;
+    const int64_t pos = L.num_rows - L.num_heavy + h;
+    const int32_t e0 = __ldg(L.row_ptr + pos);
+    const int32_t e1 = __ldg(L.row_ptr + pos + 1);
+    const int64_t row = L.row_begin + (L.row_ids ? static_cast<int64_t>(__ldg(L.row_ids + pos)) : pos);
+    const int g_lanes = 1 << a.log2g;
+    const int groups = 32 >> a.log2g;
+    const int glane = lane32 & (g_lanes - 1);
+    const int grp = lane32 >> a.log2g;
+    T* state = static_cast<T*>(a.state);
+    const int64_t step = static_cast<int64_t>(V) << a.log2g;
+    for (int64_t base = 0; base < a.k; base += step) {  // uniform trip count across the warp
+        const int64_t c = base + static_cast<int64_t>(glane) * V;
+        const bool active = c < a.k;
+        Pack<T, V> part = zero_pack<T, V>();
+        if (active) {
+            for (int32_t q = (e0 >> 2) + grp; q < (e1 >> 2); q += groups) {
+                const uint4 cq = __ldg(L.codes + q);
+                const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
+                Pack<T, V> val[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) val[u] = df_fetch<T, V>(p, code[u], c);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) add_into(part, val[u]);
+            }
+        }
+        for (int off = 16; off >= g_lanes; off >>= 1) {
+            const Pack<T, V> other = shfl_xor_pack(part, off);
+            add_into(part, other);
+        }
+        if (grp == 0 && active) {
+            Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+            add_into(acc, part);
+            st_pack(state + row * a.ld_state + c, acc);
+        }
+    }
+}
+
+template <typename T, int V, int INIT>
+__global__ void __launch_bounds__(kDfThreads, 4) dataflow_kernel(const __grid_constant__ DfArgs p) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int32_t t0 = 0;
+        if (lane == 0) t0 = df_aborted(p) ? p.total_tasks : atomicAdd(p.sync, kDfGrab);
+        t0 = __shfl_sync(kFullMask, t0, 0);
+        if (t0 >= p.total_tasks) return;
+        const int32_t t1 = min(t0 + kDfGrab, p.total_tasks);
+        for (int32_t t = t0; t < t1; ++t) {
+            int lo = 0, hi = p.num_levels;  // last level whose first task is <= t
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (p.task_begin[mid] <= t) lo = mid;
+                else hi = mid;
+            }
+            const DfLevel& L = p.lv[lo];
+            const int64_t local = t - p.task_begin[lo];
+            if (local < L.num_heavy) df_heavy<T, V, INIT>(p, L, local);
+            else df_narrow<T, V, INIT>(p, L, local - L.num_heavy);
+        }
+    }
+}
+
+// Fill rows [r0, r1) of the state (ld_state columns) with the sentinel.
+template <typename T>
+__global__ void __launch_bounds__(256) sentinel_fill_kernel(T* state, int64_t n) {
+    using Bits = typename std::conditional<std::is_same<T, double>::value, unsigned long long, unsigned>::type;
+    const Bits bits = static_cast<Bits>(SentinelBits<T>::value);
+    Bits* out = reinterpret_cast<Bits*>(state);
+    for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+        out[i] = bits;
+}
+
 // Up seeding of level 0: state[r] = init(r) (+ input row for samples).
 template <typename T, int V, int INIT>
 __global__ void __launch_bounds__(256) seed_up_kernel(LevelArgs a, int64_t num_samples, const int32_t* s2i, int32_t by_ind) {
@@ -1250,6 +1488,8 @@ int validate_common(const grg_b200_traverse_args* a) {
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
     if (a->heavy_variant < 0 || a->heavy_variant > 2) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 2]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
+    if (a->schedule != GRG_B200_SCHEDULE_LEVELS && a->schedule != GRG_B200_SCHEDULE_DATAFLOW)
+        return fail(GRG_B200_ERR_INVALID, "unknown schedule %d", a->schedule);
     if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
     if (a->init_mode == GRG_B200_INIT_XTX && !a->xtx_node) return fail(GRG_B200_ERR_INVALID, "xtx_node is NULL");
     if (a->init_mode == GRG_B200_INIT_MATRIX && (!a->init_matrix || !a->node_perm || a->ld_init < a->k))
@@ -1300,31 +1540,58 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
 template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    if (variant == 6 && heavy_variant == 2 && !exact) {
+    const bool padded_variant = variant == 6 || variant == 7;
+    if (padded_variant && heavy_variant == 2 && !exact) {
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
         const int lg = la.log2g + la.log2s;
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
+#define GRG_FUSED_MB(INIT, MB)                                                                                 \
+    if (la.log2s > 0) level_fused_kernel<T, V, INIT, true, MB><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); \
+    else level_fused_kernel<T, V, INIT, false, MB><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks);
+#define GRG_FUSED(INIT)              \
+    if (variant == 7) {              \
+        GRG_FUSED_MB(INIT, 5)        \
+    } else {                         \
+        GRG_FUSED_MB(INIT, 6)        \
+    }
         switch (init_mode) {
-            case 0: level_fused_kernel<T, V, 0><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
-            case 1: level_fused_kernel<T, V, 1><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
-            case 2: level_fused_kernel<T, V, 2><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
-            default: level_fused_kernel<T, V, 3><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); break;
+            case 0: GRG_FUSED(0) break;
+            case 1: GRG_FUSED(1) break;
+            case 2: GRG_FUSED(2) break;
+            default: GRG_FUSED(3) break;
         }
+#undef GRG_FUSED
+#undef GRG_FUSED_MB
         GRG_LAUNCH_CHECK("level_fused_kernel");
         return GRG_B200_OK;
     }
-    if (narrow > 0 && variant == 6) {
+    if (narrow > 0 && padded_variant && la.log2s > 0) {  // split rows: the fused kernel without heavy blocks
         const int lg = la.log2g + la.log2s;
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
         switch (init_mode) {
-            case 0: level_vec_kernel<T, V, 0><<<grid, kNarrowThreads, 0, s>>>(la); break;
-            case 1: level_vec_kernel<T, V, 1><<<grid, kNarrowThreads, 0, s>>>(la); break;
-            case 2: level_vec_kernel<T, V, 2><<<grid, kNarrowThreads, 0, s>>>(la); break;
-            default: level_vec_kernel<T, V, 3><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 0: level_fused_kernel<T, V, 0, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
+            case 1: level_fused_kernel<T, V, 1, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
+            case 2: level_fused_kernel<T, V, 2, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
+            default: level_fused_kernel<T, V, 3, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
         }
+        GRG_LAUNCH_CHECK("level_fused_kernel(split)");
+    } else if (narrow > 0 && padded_variant) {
+        const int lg = la.log2g;
+        const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
+        const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
+#define GRG_VEC(INIT)                                                                   \
+    if (variant == 7) level_vec_kernel<T, V, INIT, 5><<<grid, kNarrowThreads, 0, s>>>(la); \
+    else level_vec_kernel<T, V, INIT, 6><<<grid, kNarrowThreads, 0, s>>>(la);
+        switch (init_mode) {
+            case 0: GRG_VEC(0) break;
+            case 1: GRG_VEC(1) break;
+            case 2: GRG_VEC(2) break;
+            default: GRG_VEC(3) break;
+        }
+#undef GRG_VEC
         GRG_LAUNCH_CHECK("level_vec_kernel");
     } else if (narrow > 0 && variant == 4) {
         const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
@@ -1440,13 +1707,13 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     la.heavy_rows = reinterpret_cast<const int32_t*>(base + L->off_heavy);
     la.row_ids = L->off_row_ids >= 0 ? reinterpret_cast<const int32_t*>(base + L->off_row_ids) : nullptr;
     if (L->list_align != 1 && L->list_align != 4) return fail(GRG_B200_ERR_INVALID, "list_align must be 1 or 4, got %d", L->list_align);
-    if ((a->narrow_variant == 6 || a->dtype == GRG_B200_MIXED) && L->list_align != 4)
-        return fail(GRG_B200_ERR_INVALID, "narrow_variant 6 and mixed storage need padded gather lists (list_align 4)");
+    if ((a->narrow_variant >= 6 || a->dtype == GRG_B200_MIXED) && L->list_align != 4)
+        return fail(GRG_B200_ERR_INVALID, "narrow_variants 6/7 and mixed storage need padded gather lists (list_align 4)");
     if (L->list_align == 4 && (L->off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
     la.list_align = L->list_align;
     la.num_heavy = L->num_heavy;
     la.log2s = 0;
-    if (a->exact_order == 0 && a->narrow_variant == 6 && a->dtype != GRG_B200_MIXED) {
+    if (a->exact_order == 0 && a->narrow_variant >= 6 && a->dtype != GRG_B200_MIXED) {
         if (a->narrow_split >= 0) {
             la.log2s = a->narrow_split;
         } else {  // split long rows while the level alone would not fill the GPU twice over
@@ -1611,6 +1878,89 @@ int emit_all_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t
     });
 }
 
+// Dataflow schedule: eligible when every level is resident with padded lists, the default
+// (fast) mode and a plain dtype; otherwise the traversal runs level by level.
+bool dataflow_eligible(const grg_b200_traverse_args* a) {
+    if (a->schedule != GRG_B200_SCHEDULE_DATAFLOW || !a->dataflow_sync) return false;
+    if (a->exact_order || a->dtype == GRG_B200_MIXED || a->num_levels > kDfMaxLevels) return false;
+    for (int i = 0; i < a->num_levels; ++i) {
+        const grg_b200_level& L = a->levels[i];
+        if (L.ring_slot >= 0 || L.list_align != 4 || L.num_rows >= INT32_MAX) return false;
+    }
+    return true;
+}
+
+template <typename T, int V>
+int launch_dataflow_typed(DfArgs& p, int init_mode, cudaStream_t s) {
+    int device = 0, sms = 0, per_sm = 0;
+    GRG_CUDA_TRY(cudaGetDevice(&device));
+    GRG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+#define GRG_DF(INIT)                                                                                      \
+    GRG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dataflow_kernel<T, V, INIT>, kDfThreads, 0)); \
+    dataflow_kernel<T, V, INIT><<<dim3(static_cast<unsigned>(sms * (per_sm > 0 ? per_sm : 1))), kDfThreads, 0, s>>>(p);
+    switch (init_mode) {
+        case 0: GRG_DF(0) break;
+        case 1: GRG_DF(1) break;
+        case 2: GRG_DF(2) break;
+        default: GRG_DF(3) break;
+    }
+#undef GRG_DF
+    GRG_LAUNCH_CHECK("dataflow_kernel");
+    return GRG_B200_OK;
+}
+
+int run_dataflow(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    DfArgs p;  // launch parameters (about 6 KB, copied into the launch)
+    std::memset(&p, 0, sizeof(p));
+    p.a = level_args(a, sh);
+    p.a.log2s = 0;
+    p.sync = static_cast<int32_t*>(a->dataflow_sync);
+    p.num_levels = a->num_levels;
+    int64_t tasks = 0, fill_begin = INT64_MAX, fill_end = 0;
+    const int rows_per_warp_log2 = 5 - sh.log2g;
+    for (int i = 0; i < a->num_levels; ++i) {
+        const grg_b200_level& L = a->levels[i];
+        const char* base = static_cast<const char*>(L.blob);
+        if (L.num_rows > 0 && !base) return fail(GRG_B200_ERR_INVALID, "level blob is NULL");
+        if (L.row_begin < 0 || L.row_begin + L.num_rows > a->num_nodes)
+            return fail(GRG_B200_ERR_INVALID, "level rows outside the %lld nodes", (long long)a->num_nodes);
+        if (L.list_align == 4 && (L.off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
+        DfLevel& d = p.lv[i];
+        d.row_ptr = reinterpret_cast<const int32_t*>(base + L.off_row_ptr);
+        d.codes = reinterpret_cast<const uint4*>(base + L.off_entries);
+        d.row_ids = L.off_row_ids >= 0 ? reinterpret_cast<const int32_t*>(base + L.off_row_ids) : nullptr;
+        d.row_begin = L.row_begin;
+        d.num_rows = static_cast<int32_t>(L.num_rows);
+        d.num_heavy = static_cast<int32_t>(L.num_heavy);
+        p.task_begin[i] = static_cast<int32_t>(tasks);
+        const int64_t narrow = L.num_rows - L.num_heavy;
+        tasks += L.num_heavy + ((narrow + (int64_t{1} << rows_per_warp_log2) - 1) >> rows_per_warp_log2);
+        if (L.num_rows > 0) {
+            fill_begin = L.row_begin < fill_begin ? L.row_begin : fill_begin;
+            fill_end = L.row_begin + L.num_rows > fill_end ? L.row_begin + L.num_rows : fill_end;
+        }
+    }
+    if (tasks >= INT32_MAX) return fail(GRG_B200_ERR_UNSUPPORTED, "dataflow schedule: too many tasks");
+    p.task_begin[a->num_levels] = static_cast<int32_t>(tasks);
+    p.total_tasks = static_cast<int32_t>(tasks);
+    GRG_CUDA_TRY(cudaMemsetAsync(a->dataflow_sync, 0, 4 * sizeof(int32_t), s));
+    if (fill_end > fill_begin) {
+        const int64_t n = (fill_end - fill_begin) * a->ld_state;
+        const int64_t blocks = (n + 255) / 256 < 148 * 32 ? (n + 255) / 256 : 148 * 32;
+        if (a->dtype == GRG_B200_F64)
+            sentinel_fill_kernel<double><<<static_cast<unsigned>(blocks), 256, 0, s>>>(static_cast<double*>(a->state) + fill_begin * a->ld_state, n);
+        else
+            sentinel_fill_kernel<float><<<static_cast<unsigned>(blocks), 256, 0, s>>>(static_cast<float*>(a->state) + fill_begin * a->ld_state, n);
+        GRG_LAUNCH_CHECK("sentinel_fill_kernel");
+    }
+    if (a->direction == GRG_B200_UP) {
+        const int rc = seed_up_impl(a, sh, s);
+        if (rc) return rc;
+    }
+    if (tasks == 0) return GRG_B200_OK;
+    return dispatch(a, sh, [&](auto t, auto v) { return launch_dataflow_typed<decltype(t), decltype(v)::value>(p, a->init_mode, s); });
+}
+
 // Mixed down: encoded copies of the input (and miss) rows, which the level lists read.
 int encode_down_inputs(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
     if (a->num_mutations == 0) return GRG_B200_OK;
@@ -1758,6 +2108,13 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
         }
     }
 
+    if (!any_streamed && dataflow_eligible(a)) {
+        rc = run_dataflow(a, sh, s);
+        if (rc) return rc;
+        if (a->emit_all_nodes) return emit_all_impl(a, sh, s);
+        if (a->direction == GRG_B200_UP) return output_up_impl(a, sh, s);
+        return output_down_impl(a, sh, s);
+    }
     if (a->direction == GRG_B200_UP) {
         rc = seed_up_impl(a, sh, s);
         if (rc) return rc;

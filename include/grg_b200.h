@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 7
+#define GRG_B200_ABI_VERSION 8
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -189,24 +189,39 @@ typedef struct grg_b200_traverse_args {
                                            then in-order sums; 5: as 0 with at most 32 registers
                                            per thread (8 CTAs per SM); 6: padded lists (list_align
                                            4) read 4 codes per 16-byte load, next 4 prefetched
-                                           while the current 4 rows load. */
+                                           while the current 4 rows load; 7: as 6 with 48
+                                           registers per thread (5 CTAs per SM) instead of 40. */
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
                                            reduction); 2 as 1 but in the same launch as the narrow
-                                           rows (narrow_variant 6 only; otherwise as 1).  Exact
+                                           rows (narrow_variant 6/7 only; otherwise as 1).  Exact
                                            order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of
                                            num_mutations rows and ld_state columns */
     int64_t mix_scratch_bytes;
-    int32_t narrow_split;               /* narrow_variant 6, default mode, FP64/FP32: split each narrow
+    int32_t narrow_split;               /* narrow_variant 6/7, default mode, FP64/FP32: split each narrow
                                            row over 2^narrow_split lane groups (0..3), or -1 to choose
                                            per level (long rows in levels too small to fill the GPU) */
-    int32_t reserved2;
+    int32_t schedule;                   /* grg_b200_schedule */
+    void* dataflow_sync;                /* GRG_B200_SCHEDULE_DATAFLOW: device int32[4], 16-byte aligned;
+                                           [2] holds GRG_B200_DEVICE_WAIT_TIMEOUT after a failed wait */
 } grg_b200_traverse_args;
 
-#define GRG_B200_NARROW_VARIANTS 7
+/*
+ * GRG_B200_SCHEDULE_LEVELS: one launch per level (each level waits for the previous one).
+ * GRG_B200_SCHEDULE_DATAFLOW: one persistent launch for all levels of a traversal; a row
+ * waits only for its own source rows.  Used when the call is in the default (not exact)
+ * mode, FP64/FP32, every level resident with padded lists and at most 128 levels; other
+ * calls run level by level.  The rows it writes are first filled with a NaN sentinel (a
+ * quiet NaN with payload 0x80DEADBEEF001 for FP64, 0x40DEAD for FP32): inputs holding that
+ * exact NaN make the wait time out (status GRG_B200_DEVICE_WAIT_TIMEOUT, result undefined).
+ */
+typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
+#define GRG_B200_DEVICE_WAIT_TIMEOUT 6
+
+#define GRG_B200_NARROW_VARIANTS 8
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

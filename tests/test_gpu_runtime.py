@@ -102,7 +102,7 @@ def test_up_output_aliases_down_input():
 
 
 @pytest.mark.parametrize("k", [1, 2, 3, 5, 8, 16, 33])
-@pytest.mark.parametrize("variant", [0, 4, 5, 6])
+@pytest.mark.parametrize("variant", [0, 4, 5, 6, 7])
 def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     """Integer-valued inputs are exact; real-valued inputs agree to 1e-12 (default heavy-row
     reduction) — every mode of the hot path on a 60k-node graph with random node ids.  Heavy
@@ -111,7 +111,7 @@ def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
 
     oracle = OracleGRG(synth_artifact)
-    heavy_variant = {5: 1, 6: 2}.get(variant, 0)
+    heavy_variant = {5: 1, 6: 2, 7: 2}.get(variant, 0)
     pair = B200PlanPair(plan_up=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant),
                         plan_down=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant))
     rng = np.random.default_rng(100 + k)
@@ -336,6 +336,31 @@ def test_foreign_stream_ordering(synth_artifact):
         np.testing.assert_allclose(out.cpu().numpy(), oracle.matmul(x, "up"), rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("split", [1, 2, 3, -1])
+@pytest.mark.parametrize("k", [1, 3, 8])
+def test_split_narrow_rows_against_oracle(synth_artifact, k, split):
+    """Narrow rows split over 2^split lane groups (fixed, or chosen per level): integer inputs
+    exact, real inputs within 1e-12, with init values and miss rows."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    oracle = OracleGRG(synth_artifact)
+    plan = B200Plan(narrow_variant=6, heavy_threshold=24, narrow_split=split)
+    rng = np.random.default_rng(500 + k)
+    with _runtime(_layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=B200PlanPair(plan_up=plan, plan_down=plan))) as runtime:
+        (grg,) = runtime.grgs
+        for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
+            x = _pm1(rng, (k, cols))
+            np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
+            x = rng.standard_normal((k, cols))
+            init = rng.standard_normal(k)
+            np.testing.assert_allclose(grg.matmul(x, direction, init=init), oracle.matmul(x, direction, init=init),
+                                       rtol=1e-12, atol=1e-9)
+        xd, miss = rng.standard_normal((k, grg.num_mutations)), rng.standard_normal((k, grg.num_mutations))
+        np.testing.assert_allclose(grg.matmul(xd, "down", miss=miss.copy()), oracle.matmul(xd, "down", miss=miss.copy()),
+                                   rtol=1e-12, atol=1e-9)
+        assert runtime.device_error() == 0
+
+
 def test_autotune_picks_a_known_variant_and_stays_exact(synth_artifact):
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
 
@@ -350,3 +375,76 @@ def test_autotune_picks_a_known_variant_and_stays_exact(synth_artifact):
         for direction, cols in (("up", grg.num_samples), ("down", grg.num_mutations)):
             x = _pm1(rng, (4, cols))
             np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
+
+
+@pytest.mark.parametrize("variant", [6, 7])
+@pytest.mark.parametrize("k", [1, 3, 8, 33])
+def test_dataflow_schedule_matches_levels_and_oracle(synth_artifact, k, variant):
+    """The persistent dataflow traversal gives bit-identical results to the level-by-level
+    launches of the same plan (same per-row arithmetic) and matches the oracle."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(700 + k)
+    results = {}
+    inputs = {}
+    for schedule in ("levels", "dataflow"):
+        plan = B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=2, narrow_split=0, schedule=schedule)
+        with _runtime(_layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=B200PlanPair(plan_up=plan, plan_down=plan))) as runtime:
+            (grg,) = runtime.grgs
+            if not inputs:
+                inputs = {"up": rng.standard_normal((k, grg.num_samples)), "down": rng.standard_normal((k, grg.num_mutations)),
+                          "miss": rng.standard_normal((k, grg.num_mutations)), "pm1": _pm1(rng, (k, grg.num_samples)),
+                          "init": rng.standard_normal(k)}
+            out = {
+                "up": grg.matmul(inputs["up"], "up"),
+                "down": grg.matmul(inputs["down"], "down", miss=inputs["miss"].copy()),
+                "pm1": grg.matmul(inputs["pm1"], "up"),
+                "init": grg.matmul(inputs["up"], "up", init=inputs["init"]),
+                "xtx": grg.matmul(inputs["down"], "down", init="xtx"),
+            }
+            for _ in range(2):  # prepared op replayed (graph) keeps giving the same answer
+                op = grg.prepare_matmul_cuda(direction="up", k=k)
+                op.input.copy_(torch.from_numpy(inputs["up"]))
+                op()
+                np.testing.assert_array_equal(op.output.cpu().numpy(), out["up"])
+            assert runtime.device_error() == 0
+            results[schedule] = out
+    for key in results["levels"]:
+        np.testing.assert_array_equal(results["dataflow"][key], results["levels"][key], err_msg=key)
+    np.testing.assert_array_equal(results["dataflow"]["pm1"], oracle.matmul(inputs["pm1"], "up"))
+    np.testing.assert_allclose(results["dataflow"]["down"], oracle.matmul(inputs["down"], "down", miss=inputs["miss"].copy()),
+                               rtol=1e-12, atol=1e-9)
+
+
+def test_dataflow_wait_times_out_with_a_status_instead_of_hanging(synth_artifact):
+    """A traversal whose levels omit one level leaves that level's rows holding the readiness
+    sentinel; rows that read them must give up after the bounded wait, report
+    GRG_B200_DEVICE_WAIT_TIMEOUT, and leave the context usable for the next call."""
+    import ctypes
+
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+    from grg_spmv_b200.backends.b200 import _native as nat
+
+    plan = B200Plan(narrow_variant=6, heavy_threshold=24, heavy_variant=2, schedule="dataflow")
+    with _runtime(_layout([synth_artifact], requirements=_req(k=2), pair=B200PlanPair(plan_up=plan, plan_down=plan)),
+                  use_graphs=False) as runtime:
+        (grg,) = runtime.grgs
+        x = _pm1(np.random.default_rng(1), (2, grg.num_samples))
+        good = grg.matmul(x, "up")
+        op = grg.prepare_matmul_cuda(direction="up", k=2)
+        args = nat.TraverseArgs.from_buffer_copy(op._args)
+        levels = runtime._artifacts[0].levels[op._spec.direction]
+        assert levels.count >= 3
+        kept = (nat.Level * (levels.count - 1))(*([levels.array[0]] + list(levels.array[2:])))  # level 2 onward never sees level 1
+        args.levels = ctypes.cast(kept, ctypes.POINTER(nat.Level))
+        args.num_levels = levels.count - 1
+        op.input.copy_(torch.from_numpy(x))
+        stream = ctypes.c_void_p(runtime.stream_ptr)
+        nat.check(runtime._lib, runtime._lib.grg_b200_traverse(ctypes.byref(args), stream), "grg_b200_traverse")
+        torch.cuda.synchronize()
+        assert int(runtime._df_sync[2].item()) == nat.DEVICE_WAIT_TIMEOUT
+        assert runtime.device_error() == nat.DEVICE_WAIT_TIMEOUT
+        # the context is still usable and the next complete traversal is right
+        np.testing.assert_array_equal(grg.matmul(x, "up"), good)
+        assert int(runtime._df_sync[2].item()) == 0
