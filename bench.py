@@ -60,6 +60,9 @@ def parse_args():
                    help="skip the batched / mixed-precision comparison on uneven RHS blocks (runs at N=1 only)")
     p.add_argument("--tier-blocks", default="1,3,16,64,256", help="RHS block widths of the tier comparison")
     p.add_argument("--tier-steps", type=int, default=3)
+    p.add_argument("--tier-grgs", type=int, default=8, help="graphs of the multi-graph tier (0: skip it)")
+    p.add_argument("--tier-scale", type=float, default=0.5, help="size of the multi-graph tier's graphs vs 5M-40M edges")
+    p.add_argument("--tier-artifacts", default=None, help="directory for (reused) multi-graph tier artifacts")
     p.add_argument("--no-clocks", action="store_true", help="skip clock sampling and its untimed busy loops")
     p.add_argument("--artifact", default=None, help=".grg_spmv to use (generated there first if missing)")
     p.add_argument("--heavy-threshold", type=int, default=None)
@@ -163,6 +166,23 @@ def measured_peak_hbm() -> tuple[float, str]:
         except (KeyError, ValueError):
             pass
     return 6650.0, "fallback"
+
+
+def profiled_traffic(num_edges: int, k: int, precision: str, schedule: str):
+    """DRAM bytes per step of the level kernels, from the ncu summary committed under
+    profiles/ (measured on the medium graph at k = 8, FP64, per-level schedule, L2 kept warm)
+    and scaled by edges; None for other configurations."""
+    path = REPO / "profiles" / "level_traffic_medium_k8.md"
+    if k != 8 or precision != "plain" or schedule != "levels" or not path.exists():
+        return None, None
+    text = path.read_text()
+    import re
+
+    t = re.search(r"traffic_per_step_bytes_medium: (\d+)", text)
+    e = re.search(r"edges_medium: (\d+)", text)
+    if not t or not e:
+        return None, None
+    return int(t.group(1)) * num_edges / int(e.group(1)), f"{path.relative_to(REPO)} (medium graph, scaled by edges)"
 
 
 def level_units(scan, direction: str, level: int, use_miss: bool) -> tuple[int, int]:
@@ -389,17 +409,18 @@ def run_b200(args) -> None:
     cpu = None
     max_rel = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sys.path.insert(0, str(REPO / "oracle"))
-        from grg_oracle import OracleGRG
-
-        oracle = OracleGRG(path)
-        t0 = time.perf_counter()
-        ref_up = oracle.matmul(x_up_np, "up")
-        ref_down = oracle.matmul(ref_up, "down", miss=miss_np.copy())
-        cpu_s = time.perf_counter() - t0
-        cpu = {"value": 2.0 * E * k / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"1 up+down step (k={k}) of the same graph; SciPy ReferenceRuntime restatement, 1 thread",
-               "seconds": cpu_s}
+        workers = min(k, os.cpu_count() or 1)
+        pool = ParallelOracle(path, workers)
+        try:
+            pool.step(x_up_np, miss_np)  # warm-up: workers load the graph
+            t0 = time.perf_counter()
+            ref_up, ref_down = pool.step(x_up_np, miss_np)
+            cpu_s = time.perf_counter() - t0
+        finally:
+            pool.close()
+        cpu = {"value": 2.0 * E * k / cpu_s, "unit": UNIT, "cores": workers, "kind": "port",
+               "sample": f"1 up+down step (k={k}) of the same graph; SciPy ReferenceRuntime restatement, "
+                         f"{workers} processes x 1 thread (RHS columns split)", "seconds": cpu_s}
         with torch.cuda.device(device), torch.cuda.stream(stream):
             up.input.copy_(x_up)
             up()
@@ -417,7 +438,15 @@ def run_b200(args) -> None:
     torch.cuda.empty_cache()
     tiers = None
     if world == 1 and not args.no_tiers:
-        tiers = measure_tiers(args, path, device, stream)
+        tiers = {"single_graph": measure_tiers(args, [path], device, stream)}
+        torch.cuda.empty_cache()
+        if args.tier_grgs > 0:
+            t0 = time.perf_counter()
+            multi = make_multi_artifacts(args)
+            gen_multi = time.perf_counter() - t0
+            tiers["multi_graph"] = measure_tiers(args, multi, device, stream)
+            tiers["multi_graph"]["generate_s"] = gen_multi
+    traffic, traffic_src = profiled_traffic(E, k, args.precision, pair.plan_down.schedule)
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -445,7 +474,8 @@ def run_b200(args) -> None:
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
                        "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
+                         "traffic": traffic, "traffic_unit": "bytes per up+down step (level kernels)",
+                         "traffic_source": traffic_src, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
                                     if pair.plan_down.schedule == "dataflow" else
                                     "level gathers (one fused narrow+heavy launch per level)"),
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
@@ -463,12 +493,43 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
 
 
-def measure_tiers(args, path, device, stream) -> dict:
-    """Uneven RHS blocks on the same graph, three ways, same work (sum of blocks, up and down):
-    the plain FP64 drop-in (one prepared op per block and direction, one after another), a
-    plain FP64 batch (one CUDA graph, merged and tiled, autotuned) and a mixed-precision batch.
-    Device time with CUDA events; errors of each batch against the FP64 drop-in's outputs and,
-    for the blocks of width <= 3, against the CPU oracle."""
+def multi_grg_specs(count: int, scale: float):
+    """``count`` GRGs of the batching configuration's shape (5M-40M edges and 20k-400k
+    mutations, evenly spread) from the same generator, each scaled by ``scale``."""
+    from grg_spmv_b200.synth import SynthSpec
+
+    specs = []
+    for i in range(count):
+        f = i / max(count - 1, 1)
+        edges = (5e6 + f * 35e6) * scale
+        nodes = int(edges / 11.8)  # the generator's edges per node at 40 levels
+        specs.append(SynthSpec(num_samples=max(2000, nodes // 50), num_levels=40, num_nodes=nodes,
+                               num_mutations=int((20_000 + f * 380_000) * scale), children=(2, 22),
+                               miss_fraction=0.01, seed=1000 + i))
+    return specs
+
+
+def make_multi_artifacts(args) -> list[Path]:
+    from grg_spmv_b200.synth import write_synthetic_artifact
+
+    root = Path(args.tier_artifacts) if args.tier_artifacts else Path(tempfile.mkdtemp(prefix="grg_tiers_"))
+    root.mkdir(parents=True, exist_ok=True)
+    paths = []
+    for i, spec in enumerate(multi_grg_specs(args.tier_grgs, args.tier_scale)):
+        path = root / f"multi_{args.tier_scale:g}_{i}.grg_spmv"
+        if not path.exists():
+            write_synthetic_artifact(spec, path)
+        paths.append(path)
+    return paths
+
+
+def measure_tiers(args, paths, device, stream) -> dict:
+    """Uneven RHS blocks on every graph of ``paths``, three ways, same work (sum of blocks, up
+    and down, every graph): the plain FP64 drop-in (one prepared op per block, direction and
+    graph, one after another), a plain FP64 batch (one CUDA graph: blocks of a graph merged and
+    tiled, graphs on concurrent streams, autotuned) and a mixed-precision batch.  Device time
+    with CUDA events; errors of each batch against the FP64 drop-in's outputs and, for the
+    blocks of width <= 3 on the first graph, against the CPU oracle."""
     import torch
 
     from grg_spmv_b200 import RuntimeRequirements
@@ -478,21 +539,24 @@ def measure_tiers(args, path, device, stream) -> dict:
     kmax = max(blocks)
     req = RuntimeRequirements(max_k_up=kmax, max_k_down=kmax, need_down_miss_input=True, need_up_miss_output=False,
                               need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
-    layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
-                              device=device.index or 0, stream=stream)
+    layout = plan_b200_layout(artifacts=[str(p) for p in paths], dtype=np.float64, requirements=req, vram_budget_bytes=0,
+                              ring_buffer_size=0, device=device.index or 0, stream=stream)
     rng = np.random.default_rng(7)
     rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(float(np.max(np.abs(ref))), 1e-300))
     out = {"blocks": blocks, "steps": args.tier_steps, "warmup": max(args.warmup, 3)}
     with B200Runtime(layout) as rt, torch.cuda.device(device), torch.cuda.stream(stream):
-        (g,) = rt.grgs
-        E = g.num_edges
-        items = [(g, "up", kb) for kb in blocks] + [(g, "down", kb, True) for kb in blocks]
+        items = []
+        for g in rt.grgs:
+            items += [(g, "up", kb) for kb in blocks] + [(g, "down", kb, True) for kb in blocks]
         xs, misses = [], []
         for it in items:
+            g = it[0]
             cols = g.num_samples if it[1] == "up" else g.num_mutations
             xs.append(torch.from_numpy(rng.standard_normal((it[2], cols))).to(device))
             misses.append(torch.from_numpy(rng.standard_normal((it[2], g.num_mutations))).to(device) if it[1] == "down" else None)
-        work = 2.0 * E * sum(blocks)
+        work = 2.0 * sum(g.num_edges for g in rt.grgs) * sum(blocks)
+        out["graphs"] = [{"num_edges": g.num_edges, "num_nodes": g.num_nodes, "num_mutations": g.num_mutations}
+                         for g in rt.grgs]
 
         def timed(step) -> float:
             for _ in range(max(args.warmup, 3)):
@@ -507,7 +571,7 @@ def measure_tiers(args, path, device, stream) -> dict:
             return a.elapsed_time(b) / args.tier_steps
 
         # 1) plain FP64 drop-in: one prepared op per block and direction.
-        ops = [g.prepare_matmul_cuda(direction=it[1], k=it[2], use_miss=it[1] == "down") for it in items]
+        ops = [it[0].prepare_matmul_cuda(direction=it[1], k=it[2], use_miss=it[1] == "down") for it in items]
         plain_out = [None] * len(items)
 
         def dropin_step(keep=False):
@@ -540,12 +604,12 @@ def measure_tiers(args, path, device, stream) -> dict:
                 out[name] = {"value": work / (ms_b / 1e3), "ms_per_step": ms_b, "tile_k": batch.tile_k,
                              "tiles": batch.num_tiles, "tuned_ms": {str(k): v for k, v in batch.tuned_ms.items()},
                              "max_rel_err_vs_plain_f64": max(errs), "speedup_vs_dropin": ms / ms_b}
-                small = [i for i, it in enumerate(items) if it[2] <= 3]
+                small = [i for i, it in enumerate(items) if it[2] <= 3 and it[0] is rt.grgs[0]]
                 if small and not args.no_cpu_baseline:
                     sys.path.insert(0, str(REPO / "oracle"))
                     from grg_oracle import OracleGRG
 
-                    oracle = OracleGRG(path)
+                    oracle = OracleGRG(paths[0])
                     oerr, perr = [], []
                     for i in small:
                         x_np = xs[i].cpu().numpy()
@@ -556,45 +620,84 @@ def measure_tiers(args, path, device, stream) -> dict:
                     out[name]["max_rel_err_vs_oracle_blocks_le3"] = max(oerr)
                     out["plain_f64_dropin"]["max_rel_err_vs_oracle_blocks_le3"] = max(perr)
             torch.cuda.empty_cache()
-    out["workload"] = (f"same graph; RHS blocks {blocks} in both directions (down with miss rows), "
-                       f"inputs copied into the op/batch buffers every step")
+    out["workload"] = (f"{len(paths)} graph(s); RHS blocks {blocks} in both directions on each (down with miss "
+                       f"rows), inputs copied into the op/batch buffers every step")
     return out
 
 
+_WORKER_ORACLE = None
+
+
+def _oracle_worker_init(path: str) -> None:
+    global _WORKER_ORACLE
+    sys.path.insert(0, str(REPO / "oracle"))
+    from grg_oracle import OracleGRG
+
+    _WORKER_ORACLE = OracleGRG(path)
+
+
+def _oracle_worker_step(task):
+    x, miss = task
+    mid = _WORKER_ORACLE.matmul(x, "up")
+    return mid, _WORKER_ORACLE.matmul(mid, "down", miss=miss.copy())
+
+
+class ParallelOracle:
+    """The oracle (the reference's single-threaded ReferenceRuntime arithmetic) on all host
+    cores: right-hand-side columns are independent, so each of ``workers`` spawned processes
+    runs the reference algorithm on a slice of the columns."""
+
+    def __init__(self, path, workers: int) -> None:
+        import multiprocessing
+
+        self.workers = max(1, int(workers))
+        self.pool = multiprocessing.get_context("spawn").Pool(self.workers, initializer=_oracle_worker_init,
+                                                              initargs=(str(path),))
+
+    def step(self, x: np.ndarray, miss: np.ndarray):
+        parts = [p for p in np.array_split(np.arange(x.shape[0]), min(self.workers, x.shape[0])) if p.size]
+        res = self.pool.map(_oracle_worker_step, [(x[p], miss[p]) for p in parts])
+        return np.concatenate([r[0] for r in res]), np.concatenate([r[1] for r in res])
+
+    def close(self) -> None:
+        self.pool.close()
+        self.pool.join()
+
+
 def run_reference(args) -> None:
-    """The reference's CPU path (oracle port of ReferenceRuntime) on the same workload."""
+    """The reference's CPU path (oracle port of ReferenceRuntime) on the same workload, on all
+    host cores (one process per right-hand-side column, up to the core count)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, str(REPO / "oracle"))
-    from grg_oracle import OracleGRG
-
     path, _ = make_artifact(args, 0)
-    oracle = OracleGRG(path)
+    with np.load(path) as data:
+        S, M, E = (int(np.asarray(data[key]).item()) for key in ("num_samples", "num_mutations", "num_edges"))
     k = int(args.k)
+    workers = min(k, os.cpu_count() or 1)
     rng = np.random.default_rng(100)
-    x = rng.standard_normal((k, oracle.num_samples))
-    miss = rng.choice(np.asarray([0.0, 1.0]), size=(k, oracle.num_mutations), p=[0.99, 0.01])
-
-    def step():
-        mid = oracle.matmul(x, "up")
-        oracle.matmul(mid, "down", miss=miss.copy())
-
-    for _ in range(max(args.warmup, 0)):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    secs = time.perf_counter() - t0
-    value = args.steps * 2.0 * oracle.num_edges * k / secs
+    x = rng.standard_normal((k, S))
+    miss = rng.choice(np.asarray([0.0, 1.0]), size=(k, M), p=[0.99, 0.01])
+    oracle = ParallelOracle(path, workers)
+    try:
+        for _ in range(max(args.warmup, 1)):  # the first step also waits for the workers to load the graph
+            oracle.step(x, miss)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            oracle.step(x, miss)
+        secs = time.perf_counter() - t0
+    finally:
+        oracle.close()
+    value = args.steps * 2.0 * E * k / secs
+    sample = (f"full up+down steps (k={k}) of the same graph; SciPy restatement of ReferenceRuntime, "
+              f"{workers} processes x 1 thread, RHS columns split across them")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}", "k": k, "num_edges": oracle.num_edges},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": "full up+down steps; SciPy restatement of ReferenceRuntime (single-threaded)"},
+        "config": {"workload": f"{args.workload}", "k": k, "num_edges": E},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

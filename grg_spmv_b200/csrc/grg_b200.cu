@@ -763,10 +763,89 @@ __device__ __forceinline__ bool mx_entry(const LevelArgs& a, uint32_t code, cons
     return true;
 }
 
+// Generic VM-column pieces of the mixed level kernels (VM = 4: 16-byte hi + 8-byte lo loads;
+// VM = 2: 8-byte hi + 4-byte lo loads, half the registers per lane, twice the lanes per row).
+template <int VM>
+struct MxRaw;
+template <>
+struct MxRaw<4> {
+    float4 h;
+    short4 l;
+};
+template <>
+struct MxRaw<2> {
+    float2 h;
+    short2 l;
+};
+
+template <int VM>
+__device__ __forceinline__ MxRaw<VM> mx_ld(const float* hi, const short* lo) {
+    if constexpr (VM == 4)
+        return MxRaw<4>{__ldg(reinterpret_cast<const float4*>(hi)), __ldg(reinterpret_cast<const short4*>(lo))};
+    else
+        return MxRaw<2>{__ldg(reinterpret_cast<const float2*>(hi)), __ldg(reinterpret_cast<const short2*>(lo))};
+}
+
+template <int VM>
+__device__ __forceinline__ MxRaw<VM> mx_zero() {
+    if constexpr (VM == 4) return MxRaw<4>{make_float4(0.f, 0.f, 0.f, 0.f), make_short4(0, 0, 0, 0)};
+    else return MxRaw<2>{make_float2(0.f, 0.f), make_short2(0, 0)};
+}
+
+template <int VM>
+__device__ __forceinline__ void mx_add(Pack<double, VM>& a, const MxRaw<VM>& r) {
+    a.v[0] = a.v[0] + mx_decode(r.h.x, r.l.x);
+    a.v[1] = a.v[1] + mx_decode(r.h.y, r.l.y);
+    if constexpr (VM == 4) {
+        a.v[2] = a.v[2] + mx_decode(r.h.z, r.l.z);
+        a.v[3] = a.v[3] + mx_decode(r.h.w, r.l.w);
+    }
+}
+
+template <int VM>
+__device__ __forceinline__ void mx_st(float* hi, short* lo, const Pack<double, VM>& v) {
+    if constexpr (VM == 4) {
+        mx_store(hi, lo, Quad{{v.v[0], v.v[1], v.v[2], v.v[3]}});
+    } else {
+        float2 h;
+        short2 l;
+        mx_encode(v.v[0], h.x, l.x);
+        mx_encode(v.v[1], h.y, l.y);
+        *reinterpret_cast<float2*>(hi) = h;
+        *reinterpret_cast<short2*>(lo) = l;
+    }
+}
+
+template <int VM>
+__device__ __forceinline__ Pack<double, VM> f64_ld_guarded(const double* row, int64_t c, int64_t k) {
+    Pack<double, VM> q;
+#pragma unroll
+    for (int i = 0; i < VM; ++i) q.v[i] = c + i < k ? __ldg(row + c + i) : 0.0;
+    return q;
+}
+
+template <int INIT, int VM>
+__device__ __forceinline__ Pack<double, VM> mx_init_v(const LevelArgs& a, int64_t row, int64_t c) {
+    if constexpr (INIT == GRG_B200_INIT_VECTOR) {
+        return f64_ld_guarded<VM>(static_cast<const double*>(a.init_vector), c, a.k);
+    } else if constexpr (INIT == GRG_B200_INIT_XTX) {
+        return splat<double, VM>(__ldg(static_cast<const double*>(a.xtx_node) + row));
+    } else if constexpr (INIT == GRG_B200_INIT_MATRIX) {
+        const int64_t orig = __ldg(a.node_perm + row);
+        if (a.err && (orig < 0 || orig >= a.lim_state)) {
+            report(a.err, kErrPerm);
+            return zero_pack<double, VM>();
+        }
+        return f64_ld_guarded<VM>(static_cast<const double*>(a.init_matrix) + orig * a.ld_init, c, a.k);
+    } else {
+        return zero_pack<double, VM>();
+    }
+}
+
 // Narrow rows of padded lists in mixed storage: the ownership and code prefetch of
-// level_vec_kernel with 4 columns per lane; adds in list order, segment by segment.
-template <int INIT>
-__global__ void __launch_bounds__(kNarrowThreads, 3) level_mx_kernel(LevelArgs a) {
+// level_vec_kernel with VM columns per lane; adds in list order, segment by segment.
+template <int INIT, int VM>
+__global__ void __launch_bounds__(kNarrowThreads, VM == 4 ? 3 : 5) level_mx_kernel(LevelArgs a) {
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy;
@@ -779,41 +858,41 @@ __global__ void __launch_bounds__(kNarrowThreads, 3) level_mx_kernel(LevelArgs a
     const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
     const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
     const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
-    const int64_t step = static_cast<int64_t>(4) << a.log2g;
-    for (int64_t c = static_cast<int64_t>(glane) * 4; c < a.k; c += step) {
-        Quad acc = mx_init<INIT>(a, row, c);
-        Quad seg = zero_quad();
+    const int64_t step = static_cast<int64_t>(VM) << a.log2g;
+    for (int64_t c = static_cast<int64_t>(glane) * VM; c < a.k; c += step) {
+        Pack<double, VM> acc = mx_init_v<INIT, VM>(a, row, c);
+        Pack<double, VM> seg = zero_pack<double, VM>();
         const int32_t q1 = e1 >> 2;
         int32_t q = e0 >> 2;
         uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
         for (; q < q1; ++q) {
             const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
             const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
-            RawQuad val[4];
+            MxRaw<VM> val[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 const float* hi = nullptr;
                 const short* lo = nullptr;
-                val[u] = mx_entry(a, code[u], hi, lo) ? mx_load_raw(hi + c, lo + c) : zero_raw();
+                val[u] = mx_entry(a, code[u], hi, lo) ? mx_ld<VM>(hi + c, lo + c) : mx_zero<VM>();
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
                 if (code[u] & GRG_B200_SEG_START) {
-                    add_quad(acc, seg);
-                    seg = zero_quad();
+                    add_into(acc, seg);
+                    seg = zero_pack<double, VM>();
                 }
-                add_raw(seg, val[u]);  // skipped entries decode to +0
+                mx_add<VM>(seg, val[u]);  // skipped entries decode to +0
             }
             cur = nxt;
         }
-        add_quad(acc, seg);
+        add_into(acc, seg);
         const int64_t off = row * a.ld_state + c;
-        mx_store(static_cast<float*>(a.state) + off, static_cast<short*>(a.state_lo) + off, acc);
+        mx_st<VM>(static_cast<float*>(a.state) + off, static_cast<short*>(a.state_lo) + off, acc);
     }
 }
 
 // Heavy rows in mixed storage, one warp each (as level_warp_kernel, padded lists).
-template <int INIT>
+template <int INIT, int VM>
 __global__ void __launch_bounds__(kWarpRowThreads) level_mx_warp_kernel(LevelArgs a) {
     const int64_t w = static_cast<int64_t>(blockIdx.x) * (kWarpRowThreads / 32) + (threadIdx.x >> 5);
     if (w >= a.num_heavy) return;  // warp-uniform
@@ -827,35 +906,35 @@ __global__ void __launch_bounds__(kWarpRowThreads) level_mx_warp_kernel(LevelArg
     const int glane = lane32 & (g_lanes - 1);
     const int grp = lane32 >> a.log2g;
     const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
-    const int64_t step = static_cast<int64_t>(4) << a.log2g;
+    const int64_t step = static_cast<int64_t>(VM) << a.log2g;
     for (int64_t base = 0; base < a.k; base += step) {  // uniform trip count across the warp
-        const int64_t c = base + static_cast<int64_t>(glane) * 4;
+        const int64_t c = base + static_cast<int64_t>(glane) * VM;
         const bool active = c < a.k;
-        Quad part = zero_quad();
+        Pack<double, VM> part = zero_pack<double, VM>();
         if (active) {
             for (int32_t q = (e0 >> 2) + grp; q < (e1 >> 2); q += groups) {
                 const uint4 cq = __ldg(codes4 + q);
                 const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
-                RawQuad val[4];
+                MxRaw<VM> val[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const float* hi = nullptr;
                     const short* lo = nullptr;
-                    val[u] = mx_entry(a, code[u], hi, lo) ? mx_load_raw(hi + c, lo + c) : zero_raw();
+                    val[u] = mx_entry(a, code[u], hi, lo) ? mx_ld<VM>(hi + c, lo + c) : mx_zero<VM>();
                 }
 #pragma unroll
-                for (int u = 0; u < 4; ++u) add_raw(part, val[u]);
+                for (int u = 0; u < 4; ++u) mx_add<VM>(part, val[u]);
             }
         }
         for (int off = 16; off >= g_lanes; off >>= 1) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) part.v[i] = part.v[i] + __shfl_xor_sync(kFullMask, part.v[i], off);
+            const Pack<double, VM> other = shfl_xor_pack(part, off);
+            add_into(part, other);
         }
         if (grp == 0 && active) {
-            Quad acc = mx_init<INIT>(a, row, c);
-            add_quad(acc, part);
+            Pack<double, VM> acc = mx_init_v<INIT, VM>(a, row, c);
+            add_into(acc, part);
             const int64_t o = row * a.ld_state + c;
-            mx_store(static_cast<float*>(a.state) + o, static_cast<short*>(a.state_lo) + o, acc);
+            mx_st<VM>(static_cast<float*>(a.state) + o, static_cast<short*>(a.state_lo) + o, acc);
         }
     }
 }
@@ -1652,16 +1731,17 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     return GRG_B200_OK;
 }
 
-int launch_level_mx(const LevelArgs& la, int init_mode, cudaStream_t s) {
+template <int VM>
+int launch_level_mx_typed(const LevelArgs& la, int init_mode, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     if (narrow > 0) {
         const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
         switch (init_mode) {
-            case 0: level_mx_kernel<0><<<grid, kNarrowThreads, 0, s>>>(la); break;
-            case 1: level_mx_kernel<1><<<grid, kNarrowThreads, 0, s>>>(la); break;
-            case 2: level_mx_kernel<2><<<grid, kNarrowThreads, 0, s>>>(la); break;
-            default: level_mx_kernel<3><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 0: level_mx_kernel<0, VM><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 1: level_mx_kernel<1, VM><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            case 2: level_mx_kernel<2, VM><<<grid, kNarrowThreads, 0, s>>>(la); break;
+            default: level_mx_kernel<3, VM><<<grid, kNarrowThreads, 0, s>>>(la); break;
         }
         GRG_LAUNCH_CHECK("level_mx_kernel");
     }
@@ -1669,14 +1749,24 @@ int launch_level_mx(const LevelArgs& la, int init_mode, cudaStream_t s) {
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
         switch (init_mode) {
-            case 0: level_mx_warp_kernel<0><<<grid, kWarpRowThreads, 0, s>>>(la); break;
-            case 1: level_mx_warp_kernel<1><<<grid, kWarpRowThreads, 0, s>>>(la); break;
-            case 2: level_mx_warp_kernel<2><<<grid, kWarpRowThreads, 0, s>>>(la); break;
-            default: level_mx_warp_kernel<3><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 0: level_mx_warp_kernel<0, VM><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 1: level_mx_warp_kernel<1, VM><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 2: level_mx_warp_kernel<2, VM><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            default: level_mx_warp_kernel<3, VM><<<grid, kWarpRowThreads, 0, s>>>(la); break;
         }
         GRG_LAUNCH_CHECK("level_mx_warp_kernel");
     }
     return GRG_B200_OK;
+}
+
+// Mixed level launches: narrow_variant 7 walks rows with 2 columns per lane, others with 4.
+int launch_level_mx(LevelArgs la, int init_mode, int variant, cudaStream_t s) {
+    const int vm = variant == 7 ? 2 : 4;
+    const int64_t cols = (la.k + vm - 1) / vm;
+    int log2g = 0;
+    while ((1 << log2g) < cols && log2g < 5) ++log2g;
+    la.log2g = log2g;
+    return vm == 2 ? launch_level_mx_typed<2>(la, init_mode, s) : launch_level_mx_typed<4>(la, init_mode, s);
 }
 
 template <typename F>
@@ -1728,7 +1818,7 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     }
     la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
     const bool exact = a->exact_order != 0;
-    if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, s);
+    if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, a->narrow_variant, s);
     return dispatch(a, sh, [&](auto t, auto v) {
         return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant, s);
     });

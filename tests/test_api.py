@@ -164,3 +164,21 @@ def test_root_import_is_cpu_safe():
     )
     out = subprocess.run([sys.executable, "-c", script], check=True, capture_output=True, text=True).stdout
     assert json.loads(out) == {"runtime": False}
+
+
+def test_capture_spec_validation_mirrors_the_reference():
+    from grg_spmv_b200 import RuntimeRequirements
+    from grg_spmv_b200.adaptor import CaptureSpec, validate_capture_spec
+
+    req = RuntimeRequirements(max_k_up=4, max_k_down=4, need_down_miss_input=False, need_up_miss_output=False,
+                              need_init_vector=False, need_init_matrix=True, need_init_xtx=False)
+    validate_capture_spec(CaptureSpec("up", 4), req)
+    validate_capture_spec(CaptureSpec("down", 4, init_mode="matrix"), req)
+    for spec, msg in ((CaptureSpec("up", 4, init_mode="bogus"), "invalid"),
+                      (CaptureSpec("up", 4, init_mode="matrix", use_miss=True), "mutually exclusive"),
+                      (CaptureSpec("up", 4, use_miss=True), "need_up_miss_output"),
+                      (CaptureSpec("down", 4, use_miss=True), "need_down_miss_input"),
+                      (CaptureSpec("up", 4, init_mode="vector"), "need_init_vector"),
+                      (CaptureSpec("up", 4, init_mode="xtx"), "need_init_xtx")):
+        with pytest.raises(ValueError, match=msg):
+            validate_capture_spec(spec, req)
