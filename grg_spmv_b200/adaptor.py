@@ -228,15 +228,19 @@ def capture_grg(grg, capture_stream, req, stack: contextlib.ExitStack, *, captur
     (and one init / miss buffer) sized for the largest spec is shared by all captures of the
     GRG, which never run concurrently (the reference's ``_capture_grg``).
 
-    ``capture_stream`` must be the runtime's stream (the layout's ``stream``), because the
-    prepared ops launch there; None uses it directly."""
+    The graphs are recorded on ``capture_stream`` (a fresh stream when None or the default
+    stream, which cannot capture) and replayed, with the staging copies, on the runtime's
+    stream (the layout's ``stream``)."""
+    import ctypes
+
     import torch
 
-    own_stream = grg._runtime._torch_caller_stream()
-    if capture_stream is None:
-        capture_stream = own_stream
-    elif int(capture_stream.cuda_stream) != int(own_stream.cuda_stream):
-        raise ValueError("capture_stream must be the runtime's stream (the layout's stream)")
+    from grg_spmv_b200.backends.b200 import _native as nat
+
+    runtime = grg._runtime
+    run_stream = runtime._torch_caller_stream()
+    if capture_stream is None or int(capture_stream.cuda_stream) == 0:
+        capture_stream = torch.cuda.Stream(device=run_stream.device)
 
     specs = tuple(capture_ops) or (CaptureSpec("up", int(req.max_k_up)), CaptureSpec("down", int(req.max_k_down)))
     prepared = {}
@@ -266,6 +270,7 @@ def capture_grg(grg, capture_stream, req, stack: contextlib.ExitStack, *, captur
         k, cols = op.input.shape
         src = torch.as_strided(shared_src, size=(k, cols), stride=(1, k))
         graph = torch.cuda.CUDAGraph()
+        capture_stream.wait_stream(run_stream)
         with torch.cuda.graph(graph, stream=capture_stream, capture_error_mode="thread_local"):
             op.input.copy_(src)
             if spec.init_mode == "vector":
@@ -277,10 +282,13 @@ def capture_grg(grg, capture_stream, req, stack: contextlib.ExitStack, *, captur
             elif spec.use_miss and spec.direction == "down":
                 misses[key] = torch.as_strided(shared_miss, size=(k, op.miss_input.shape[1]), stride=(1, k))
                 op.miss_input.copy_(misses[key])
-            op()
+            # the traversal itself, launched into this capture (the prepared op's own launch
+            # path targets the runtime's stream)
+            status = runtime._lib.grg_b200_traverse(ctypes.byref(op._args), ctypes.c_void_p(capture_stream.cuda_stream))
+        nat.check(runtime._lib, status, "grg_b200_traverse (adaptor capture)")
         srcs[key] = src
         graphs[key] = graph
-    return CapturedBoundGRG(grg, prepared, graphs, srcs, inits, misses, capture_stream, native=native,
+    return CapturedBoundGRG(grg, prepared, graphs, srcs, inits, misses, run_stream, native=native,
                             device_lock=device_lock)
 
 

@@ -96,10 +96,10 @@ class B200Plan:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
         if self.row_order not in (None, "natural", "locality"):
             raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
-        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < 8:
-            raise ValueError(f"narrow_variant must be in [0, 8), got {self.narrow_variant}")
+        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < 9:
+            raise ValueError(f"narrow_variant must be in [0, 9), got {self.narrow_variant}")
         if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
-            raise ValueError("narrow_variants 6 and 7 read padded gather lists; they need pad_lists=True")
+            raise ValueError("narrow_variants 6-8 read padded gather lists; they need pad_lists=True")
         if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2):
             raise ValueError(f"heavy_variant must be 0, 1 or 2, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:

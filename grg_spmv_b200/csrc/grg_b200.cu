@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(kAsyncThreads) level_async_kernel(LevelArgs a)
 // Narrow rows from padded lists (narrow_variant 6).  Same ownership as level_narrow_kernel; a
 // lane reads its row's codes four at a time with one aligned 16-byte load and loads the next
 // four while the current four rows are fetched, so each round waits on one memory latency.
-template <typename T, int V, int INIT>
+template <typename T, int V, int INIT, int Q = 1>
 __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -427,27 +427,39 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
         Pack<T, V> seg = zero_pack<T, V>();
         const int32_t q1 = e1 >> 2;
         int32_t q = e0 >> 2;
-        uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
-        for (; q < q1; ++q) {
-            const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
-            const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
-            Pack<T, V> val[4];
-            bool valid[4];
+        uint4 cur[Q];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+        for (int j = 0; j < Q; ++j) cur[j] = q + j < q1 ? __ldg(codes4 + q + j) : null4;
+        for (; q < q1; q += Q) {  // Q quads (4 * Q row fetches) in flight per round
+            uint4 nxt[Q];
+#pragma unroll
+            for (int j = 0; j < Q; ++j) nxt[j] = q + Q + j < q1 ? __ldg(codes4 + q + Q + j) : null4;
+            uint32_t code[4 * Q];
+#pragma unroll
+            for (int j = 0; j < Q; ++j) {
+                code[4 * j] = cur[j].x;
+                code[4 * j + 1] = cur[j].y;
+                code[4 * j + 2] = cur[j].z;
+                code[4 * j + 3] = cur[j].w;
+            }
+            Pack<T, V> val[4 * Q];
+            bool valid[4 * Q];
+#pragma unroll
+            for (int u = 0; u < 4 * Q; ++u) {
                 const T* src = entry_row<T>(a, code[u]);
                 valid[u] = src != nullptr;
                 val[u] = valid[u] ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
             }
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+            for (int u = 0; u < 4 * Q; ++u) {
                 if (code[u] & GRG_B200_SEG_START) {
                     add_into(acc, seg);
                     seg = zero_pack<T, V>();
                 }
                 if (valid[u]) add_into(seg, val[u]);
             }
-            cur = nxt;
+#pragma unroll
+            for (int j = 0; j < Q; ++j) cur[j] = nxt[j];
         }
         add_into(acc, seg);
         st_pack(state + row * a.ld_state + c, acc);
@@ -514,11 +526,12 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
     }
 }
 
-// MB = CTAs per SM the register budget is sized for: 6 (narrow_variant 6, 40 registers) or 5
-// (narrow_variant 7, 48 registers: no spills, fewer warps).
-template <typename T, int V, int INIT, int MB>
+// MB = CTAs per SM the register budget is sized for: 6 (narrow_variant 6, 40 registers), 5
+// (narrow_variant 7, 48 registers: no spills, fewer warps) or 3 (narrow_variant 8, Q = 2: two
+// quads, eight row fetches, in flight per round).
+template <typename T, int V, int INIT, int MB, int Q = 1>
 __global__ void __launch_bounds__(kNarrowThreads, MB) level_vec_kernel(LevelArgs a) {
-    vec_rows<T, V, INIT>(a, blockIdx.x);
+    vec_rows<T, V, INIT, Q>(a, blockIdx.x);
 }
 
 constexpr int kWarpRowThreads = 256;
@@ -600,12 +613,12 @@ __global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a
 // narrow rows as level_vec_kernel does.  The two kinds of rows are disjoint and read only
 // lower levels, so nothing orders them; this saves the second launch of a level and lets the
 // heavy rows overlap the narrow ones.
-template <typename T, int V, int INIT, bool SPLIT, int MB>
+template <typename T, int V, int INIT, bool SPLIT, int MB, int Q = 1>
 __global__ void __launch_bounds__(kNarrowThreads, MB) level_fused_kernel(LevelArgs a, int64_t heavy_blocks) {
     static_assert(kNarrowThreads == kWarpRowThreads, "both row kinds use the same CTA shape");
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
     else if constexpr (SPLIT) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
-    else vec_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+    else vec_rows<T, V, INIT, Q>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1619,7 +1632,7 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
 template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    const bool padded_variant = variant == 6 || variant == 7;
+    const bool padded_variant = variant >= 6 && variant <= 8;
     if (padded_variant && heavy_variant == 2 && !exact) {
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
@@ -1629,11 +1642,14 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
 #define GRG_FUSED_MB(INIT, MB)                                                                                 \
     if (la.log2s > 0) level_fused_kernel<T, V, INIT, true, MB><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); \
     else level_fused_kernel<T, V, INIT, false, MB><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks);
-#define GRG_FUSED(INIT)              \
-    if (variant == 7) {              \
-        GRG_FUSED_MB(INIT, 5)        \
-    } else {                         \
-        GRG_FUSED_MB(INIT, 6)        \
+#define GRG_FUSED(INIT)                                                                                  \
+    if (variant == 8) {                                                                                  \
+        if (la.log2s > 0) level_fused_kernel<T, V, INIT, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); \
+        else level_fused_kernel<T, V, INIT, false, 3, 2><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks);          \
+    } else if (variant == 7) {                                                                           \
+        GRG_FUSED_MB(INIT, 5)                                                                            \
+    } else {                                                                                             \
+        GRG_FUSED_MB(INIT, 6)                                                                            \
     }
         switch (init_mode) {
             case 0: GRG_FUSED(0) break;
@@ -1661,8 +1677,9 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         const int lg = la.log2g;
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
-#define GRG_VEC(INIT)                                                                   \
-    if (variant == 7) level_vec_kernel<T, V, INIT, 5><<<grid, kNarrowThreads, 0, s>>>(la); \
+#define GRG_VEC(INIT)                                                                      \
+    if (variant == 8) level_vec_kernel<T, V, INIT, 3, 2><<<grid, kNarrowThreads, 0, s>>>(la); \
+    else if (variant == 7) level_vec_kernel<T, V, INIT, 5><<<grid, kNarrowThreads, 0, s>>>(la); \
     else level_vec_kernel<T, V, INIT, 6><<<grid, kNarrowThreads, 0, s>>>(la);
         switch (init_mode) {
             case 0: GRG_VEC(0) break;

@@ -190,18 +190,20 @@ typedef struct grg_b200_traverse_args {
                                            per thread (8 CTAs per SM); 6: padded lists (list_align
                                            4) read 4 codes per 16-byte load, next 4 prefetched
                                            while the current 4 rows load; 7: as 6 with 48
-                                           registers per thread (5 CTAs per SM) instead of 40. */
+                                           registers per thread (5 CTAs per SM) instead of 40;
+                                           8: as 6 with 8 codes (two 16-byte loads) and 8 row
+                                           fetches in flight per round (3 CTAs per SM). */
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
                                            reduction); 2 as 1 but in the same launch as the narrow
-                                           rows (narrow_variant 6/7 only; otherwise as 1).  Exact
+                                           rows (narrow_variant 6/7/8 only; otherwise as 1).  Exact
                                            order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of
                                            num_mutations rows and ld_state columns */
     int64_t mix_scratch_bytes;
-    int32_t narrow_split;               /* narrow_variant 6/7, default mode, FP64/FP32: split each narrow
+    int32_t narrow_split;               /* narrow_variant 6/7/8, default mode, FP64/FP32: split each narrow
                                            row over 2^narrow_split lane groups (0..3), or -1 to choose
                                            per level (long rows in levels too small to fill the GPU) */
     int32_t schedule;                   /* grg_b200_schedule */
@@ -221,7 +223,7 @@ typedef struct grg_b200_traverse_args {
 typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
 #define GRG_B200_DEVICE_WAIT_TIMEOUT 6
 
-#define GRG_B200_NARROW_VARIANTS 8
+#define GRG_B200_NARROW_VARIANTS 9
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

@@ -102,7 +102,7 @@ def test_up_output_aliases_down_input():
 
 
 @pytest.mark.parametrize("k", [1, 2, 3, 5, 8, 16, 33])
-@pytest.mark.parametrize("variant", [0, 4, 5, 6, 7])
+@pytest.mark.parametrize("variant", [0, 4, 5, 6, 7, 8])
 def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     """Integer-valued inputs are exact; real-valued inputs agree to 1e-12 (default heavy-row
     reduction) — every mode of the hot path on a 60k-node graph with random node ids.  Heavy
@@ -111,7 +111,7 @@ def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
 
     oracle = OracleGRG(synth_artifact)
-    heavy_variant = {5: 1, 6: 2, 7: 2}.get(variant, 0)
+    heavy_variant = {5: 1, 6: 2, 7: 2, 8: 2}.get(variant, 0)
     pair = B200PlanPair(plan_up=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant),
                         plan_down=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant))
     rng = np.random.default_rng(100 + k)
