@@ -73,6 +73,7 @@ def parse_args():
     p.add_argument("--heavy-variant", type=int, default=None,
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
+    p.add_argument("--slots", action="store_true", help="pad narrow rows to their bucket width (list offset from position)")
     p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
     p.add_argument("--schedule", choices=["levels", "dataflow"], default=None,
                    help="one launch per level, or one persistent dataflow launch per traversal")
@@ -242,6 +243,8 @@ def run_b200(args) -> None:
         extra["heavy_variant"] = args.heavy_variant
     if args.short_first:
         extra["long_first"] = False
+    if args.slots:
+        extra["slots"] = True
     if args.narrow_split is not None:
         extra["narrow_split"] = args.narrow_split
     if args.schedule is not None:
@@ -467,7 +470,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "narrow_split": pair.plan_down.narrow_split,
+                       "long_first": pair.plan_down.long_first, "slots": pair.plan_down.slots, "narrow_split": pair.plan_down.narrow_split,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",

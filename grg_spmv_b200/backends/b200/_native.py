@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -28,6 +28,7 @@ NVCC_FLAGS = (
 # Status codes, enums and entry coding (grg_b200.h).
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED = 0, 1, 2, 3
 F64, F32, MIXED = 0, 1, 2
+MAX_SLOT_BUCKETS = 8
 SCHEDULE_LEVELS, SCHEDULE_DATAFLOW = 0, 1
 DEVICE_WAIT_TIMEOUT = 6
 UP, DOWN = 0, 1
@@ -73,7 +74,10 @@ class Level(ctypes.Structure):
         ("off_row_ids", ctypes.c_int64),
         ("off_entries", ctypes.c_int64),
         ("list_align", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("num_slot_buckets", ctypes.c_int32),
+        ("slot_pos", ctypes.c_int64 * 8),
+        ("slot_entry", ctypes.c_int64 * 8),
+        ("slot_width", ctypes.c_int32 * 8),
     ]
 
 

@@ -72,6 +72,9 @@ class B200Plan:
     the narrow-row launch (2, with ``narrow_variant`` 6 or 7); None picks 2 with the padded
     variants and otherwise 1 for k <= 16, 0 above.  Exact order always uses CTAs.
     ``long_first``: with ``balance``, the longest length bucket is processed first.
+    ``slots``: with ``balance`` and ``pad_lists``, pad each narrow row to its bucket's width
+    (1, 2, 4, 8 quads of 4 entries) so kernels locate its list from its position instead of
+    loading ``row_ptr`` (one dependent load fewer per row, up to twice the list bytes).
     ``narrow_split``: split each narrow row over 2^narrow_split lane groups (0..3; -1 chooses
     per level; default mode with ``narrow_variant`` 6 or 7 only).
     ``schedule``: "levels" (one launch per level) or "dataflow" (one persistent launch per
@@ -88,6 +91,7 @@ class B200Plan:
     pad_lists: bool = True
     heavy_variant: int | None = None
     long_first: bool = True
+    slots: bool = False
     narrow_split: int = -1
     schedule: str = "levels"
 
@@ -123,7 +127,7 @@ class B200Plan:
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
-                   "heavy_variant", "long_first", "narrow_split", "schedule"}
+                   "heavy_variant", "long_first", "narrow_split", "schedule", "slots"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -133,7 +137,7 @@ class B200Plan:
                    balance=bool(value.get("balance", True)), autotune=bool(value.get("autotune", False)),
                    pad_lists=bool(value.get("pad_lists", True)), heavy_variant=value.get("heavy_variant"),
                    long_first=bool(value.get("long_first", True)), narrow_split=int(value.get("narrow_split", -1)),
-                   schedule=str(value.get("schedule", "levels")))
+                   schedule=str(value.get("schedule", "levels")), slots=bool(value.get("slots", False)))
 
 
 @dataclass(frozen=True)
@@ -310,8 +314,9 @@ def _level_plans(artifact_index: int, scan: ArtifactScan, direction: Direction, 
         rows = int(scan.level_sizes[level])
         if rows == 0:
             continue
-        entries = (up_entry_bound(scan, level, plan.pad_lists) if direction == Direction.UP
-                   else down_entry_bound(scan, level, with_miss, plan.pad_lists))
+        slots = plan.slots and plan.pad_lists and plan.balance
+        entries = (up_entry_bound(scan, level, plan.pad_lists, slots) if direction == Direction.UP
+                   else down_entry_bound(scan, level, with_miss, plan.pad_lists, slots))
         heavy = min(rows, entries // (int(plan.heavy_threshold) + 1))
         nbytes = blob_layout(rows, heavy, entries, True)[4]  # row map: locality order or heavy suffix
         out.append(LevelPlan(artifact_index, direction, level, pos, rows, entries, heavy, nbytes))

@@ -290,14 +290,14 @@ class B200Runtime:
         if up_on:
             plan = lay.pair.plan_up
             built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance,
-                                                            plan.pad_lists, plan.long_first)}
+                                                            plan.pad_lists, plan.long_first, plan.slots)}
             levels[Direction.UP] = self._upload_levels(art.levels_up, built)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
             plan = lay.pair.plan_down
             built = {lv.level: lv for lv in build_down_levels(
                 off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
-                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first)}
+                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first, plan.slots)}
             levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
         del coo
         return _DeviceArtifact(
@@ -340,6 +340,10 @@ class B200Runtime:
                                num_heavy=int(lv.heavy_rows.size), heavy_threshold=lv.heavy_threshold, ring_slot=slot,
                                blob=blob.data_ptr(), blob_bytes=nbytes, off_row_ptr=off_ptr, off_heavy=off_heavy,
                                off_row_ids=off_ids, off_entries=off_entries, list_align=lv.list_align)
+            if lv.slots is not None:
+                arr[i].num_slot_buckets = int(lv.slots.shape[0])
+                for b, (pos, entry, width) in enumerate(lv.slots):
+                    arr[i].slot_pos[b], arr[i].slot_entry[b], arr[i].slot_width[b] = int(pos), int(entry), int(width)
         return _DeviceLevels(array=arr, keepalive=keep)
 
     # -- autotuning ------------------------------------------------------------------------------

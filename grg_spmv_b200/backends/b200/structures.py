@@ -60,6 +60,10 @@ class LevelGather:
     heavy_threshold: int
     row_ids: np.ndarray | None = None  # int32 level-local row of each position (None: identity)
     list_align: int = 1  # 4: lists padded to multiples of 4 entries with null codes
+    # slot layout: int64 [buckets, 3] = (first position, first entry, width in 4-entry quads);
+    # every narrow row of a bucket holds exactly `width` quads, so its list starts at
+    # first entry + (position - first position) * 4 * width
+    slots: np.ndarray | None = None
 
     @property
     def num_entries(self) -> int:
@@ -98,9 +102,18 @@ def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.nd
     return rows, cols
 
 
+def _quad_class(counts: np.ndarray) -> np.ndarray:
+    """Slot width in 4-entry quads of rows with ``counts`` entries: 0, 1, 2, 4, 8, ..."""
+    quads = (np.asarray(counts, dtype=np.int64) + 3) // 4
+    width = np.ones_like(quads)
+    while np.any(width < quads):
+        width = np.where(width < quads, width * 2, width)
+    return np.where(quads == 0, 0, width)
+
+
 def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
             group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True,
-            pad: bool = False, long_first: bool = True) -> LevelGather:
+            pad: bool = False, long_first: bool = True, slots: bool = False) -> LevelGather:
     """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr.
 
     With ``locality`` the rows are stored in the order of the id of their last state entry
@@ -133,8 +146,12 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
         uniq, first_rev = np.unique(rows[state_pos][::-1], return_index=True)
         key[uniq] = ids[state_pos[::-1][first_rev]]
         perm = np.argsort(key, kind="stable")
+    use_slots = slots and pad and balance
     if balance and num_rows > 1:
-        bucket = np.ceil(np.log2(counts[perm] + 1.0)).astype(np.int64)
+        if use_slots:  # buckets of equal padded width (power-of-two quads)
+            bucket = _quad_class(counts[perm])
+        else:
+            bucket = np.ceil(np.log2(counts[perm] + 1.0)).astype(np.int64)
         perm = perm[np.argsort(-bucket if long_first else bucket, kind="stable")]
     heavy_mask = counts[perm] > heavy_threshold
     perm = np.concatenate((perm[~heavy_mask], perm[heavy_mask]))
@@ -148,9 +165,20 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
         entries = entries[gather]
         row_ptr, row_ids = new_ptr, perm.astype(np.int32)
     counts = np.diff(row_ptr)
+    slot_table = None
     if pad:
-        # Every list starts at a multiple of 4 entries and holds a multiple of 4 (null padding).
+        # Every list starts at a multiple of 4 entries and holds a multiple of 4 (null padding);
+        # with slots a narrow row is padded to its bucket's width.
         padded = (counts + 3) // 4 * 4
+        if use_slots:
+            narrow = num_rows - num_heavy
+            width = _quad_class(counts[:narrow])
+            padded = padded.copy()
+            padded[:narrow] = 4 * width
+            starts = np.concatenate(([0], np.flatnonzero(width[1:] != width[:-1]) + 1)) if narrow else np.empty(0, np.int64)
+            first_entry = np.concatenate(([0], np.cumsum(padded[:narrow])))
+            slot_table = np.stack([starts, first_entry[starts], width[starts]], axis=1).astype(np.int64) if narrow else \
+                np.zeros((0, 3), dtype=np.int64)
         new_ptr = np.zeros(num_rows + 1, dtype=np.int64)
         np.cumsum(padded, out=new_ptr[1:])
         out = np.full(int(new_ptr[-1]), np.uint32(nat.SRC_NULL << nat.SRC_SHIFT), dtype=np.uint32)
@@ -160,8 +188,10 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
         if row_ptr[-1] > np.iinfo(np.int32).max:
             raise ValueError(f"level {level} has {int(row_ptr[-1])} padded entries, above the 2^31-1 per-level limit")
     heavy = np.arange(num_rows - num_heavy, num_rows, dtype=np.int32)
+    if slot_table is not None and slot_table.shape[0] > nat.MAX_SLOT_BUCKETS:
+        slot_table = None  # more width classes than the kernels take: row_ptr is still exact
     return LevelGather(level, int(row_begin), int(num_rows), row_ptr.astype(np.int32), entries, heavy,
-                       int(heavy_threshold), row_ids, 4 if pad else 1)
+                       int(heavy_threshold), row_ids, 4 if pad else 1, slot_table)
 
 
 def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
@@ -175,7 +205,7 @@ def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
 
 
 def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, locality: bool = False,
-                    balance: bool = True, pad: bool = False, long_first: bool = True) -> list[LevelGather]:
+                    balance: bool = True, pad: bool = False, long_first: bool = True, slots: bool = False) -> list[LevelGather]:
     """Gather lists for up levels 1..h-1 (level 0 is seeded from the input)."""
     off = np.asarray(level_offsets, dtype=np.int64)
     h = off.size - 1
@@ -192,7 +222,7 @@ def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, 
             src.append(np.full(r.size, s, dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
-        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first))
+        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first, slots))
     return levels
 
 
@@ -207,7 +237,7 @@ def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[
 
 def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int,
                       locality: bool = True, balance: bool = True, pad: bool = False,
-                      long_first: bool = True) -> list[LevelGather]:
+                      long_first: bool = True, slots: bool = False) -> list[LevelGather]:
     """Gather lists for down levels h-1..0 in execution order.
 
     ``sel_mut``/``sel_miss`` are (indptr, indices, num_mutations) triples; ``sel_miss`` may be
@@ -240,21 +270,31 @@ def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, h
             grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         levels.append(_finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
-                              cat(grp, np.int16), heavy_threshold, locality, balance, pad, long_first))
+                              cat(grp, np.int16), heavy_threshold, locality, balance, pad, long_first, slots))
     return levels
 
 
-def up_entry_bound(scan, level: int, pad: bool = False) -> int:
+def _padded_bound(total: int, rows: int, pad: bool, slots: bool) -> int:
+    """Entries after padding: multiples of 4 add < 4 per row; slot widths at most double a
+    padded narrow list (+4 per row covers the rounding)."""
+    if not pad:
+        return int(total)
+    if slots:
+        return int(2 * total + 4 * rows)
+    return int(total + 3 * rows)
+
+
+def up_entry_bound(scan, level: int, pad: bool = False, slots: bool = False) -> int:
     total = sum(b.nnz for b in scan.blocks if b.dst_level == level)
-    return int(total + (3 * scan.level_sizes[level] if pad else 0))
+    return _padded_bound(total, int(scan.level_sizes[level]), pad, slots)
 
 
-def down_entry_bound(scan, level: int, with_miss: bool, pad: bool = False) -> int:
+def down_entry_bound(scan, level: int, with_miss: bool, pad: bool = False, slots: bool = False) -> int:
     total = sum(b.nnz for b in scan.blocks if b.src_level == level)
     total += int(scan.selector_nnz_by_level[level, 0])
     if with_miss:
         total += int(scan.selector_nnz_by_level[level, 1])
-    return int(total + (3 * scan.level_sizes[level] if pad else 0))
+    return _padded_bound(total, int(scan.level_sizes[level]), pad, slots)
 
 
 __all__ = [

@@ -157,6 +157,10 @@ struct LevelArgs {
     int64_t lim_x;
     int64_t lim_miss;
     int32_t log2s;  // narrow rows split over 2^log2s lane groups (default mode, variant 6)
+    int32_t num_slot_buckets;  // > 0: narrow lists located from the slot table, not row_ptr
+    int32_t slot_width[GRG_B200_MAX_SLOT_BUCKETS];
+    int64_t slot_pos[GRG_B200_MAX_SLOT_BUCKETS];
+    int64_t slot_entry[GRG_B200_MAX_SLOT_BUCKETS];
     // mixed storage only: the 16-bit planes of state, x and miss (x/miss hold encoded copies)
     void* state_lo;
     const void* x_lo;
@@ -406,6 +410,23 @@ __global__ void __launch_bounds__(kAsyncThreads) level_async_kernel(LevelArgs a)
 // Narrow rows from padded lists (narrow_variant 6).  Same ownership as level_narrow_kernel; a
 // lane reads its row's codes four at a time with one aligned 16-byte load and loads the next
 // four while the current four rows are fetched, so each round waits on one memory latency.
+// A narrow row's list: from the slot table when the level has one (no dependent load), else
+// from row_ptr.
+__device__ __forceinline__ void narrow_extent(const LevelArgs& a, int64_t pos, int32_t& e0, int32_t& e1) {
+    if (a.num_slot_buckets > 0) {
+        int b = 0;
+#pragma unroll
+        for (int i = 1; i < GRG_B200_MAX_SLOT_BUCKETS; ++i)
+            if (i < a.num_slot_buckets && pos >= a.slot_pos[i]) b = i;
+        const int32_t w = 4 * a.slot_width[b];
+        e0 = static_cast<int32_t>(a.slot_entry[b] + (pos - a.slot_pos[b]) * w);
+        e1 = e0 + w;
+    } else {
+        e0 = __ldg(a.row_ptr + pos);
+        e1 = __ldg(a.row_ptr + pos + 1);
+    }
+}
+
 template <typename T, int V, int INIT, int Q = 1>
 __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const int warp = threadIdx.x >> 5;
@@ -413,8 +434,8 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
     const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
     if (pos >= narrow) return;  // no warp-wide operations below
-    const int32_t e0 = __ldg(a.row_ptr + pos);
-    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
+    int32_t e0, e1;
+    narrow_extent(a, pos, e0, e1);
     const int glane = lane & ((1 << a.log2g) - 1);
     const int64_t row = level_row(a, pos);
     const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
@@ -1819,6 +1840,22 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     if (L->list_align == 4 && (L->off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
     la.list_align = L->list_align;
     la.num_heavy = L->num_heavy;
+    la.num_slot_buckets = 0;
+    if (L->num_slot_buckets < 0 || L->num_slot_buckets > GRG_B200_MAX_SLOT_BUCKETS)
+        return fail(GRG_B200_ERR_INVALID, "num_slot_buckets %d outside [0, %d]", L->num_slot_buckets, GRG_B200_MAX_SLOT_BUCKETS);
+    if (L->num_slot_buckets > 0) {
+        if (L->list_align != 4 || L->slot_pos[0] != 0) return fail(GRG_B200_ERR_INVALID, "slot table needs padded lists starting at position 0");
+        for (int b = 0; b < L->num_slot_buckets; ++b) {
+            const int64_t end = b + 1 < L->num_slot_buckets ? L->slot_pos[b + 1] : L->num_rows - L->num_heavy;
+            if (L->slot_width[b] < 0 || end < L->slot_pos[b] || L->slot_entry[b] < 0 || (L->slot_entry[b] & 3) ||
+                L->slot_entry[b] + (end - L->slot_pos[b]) * 4 * L->slot_width[b] > L->num_entries)
+                return fail(GRG_B200_ERR_INVALID, "slot bucket %d outside the level's lists", b);
+            la.slot_pos[b] = L->slot_pos[b];
+            la.slot_entry[b] = L->slot_entry[b];
+            la.slot_width[b] = L->slot_width[b];
+        }
+        la.num_slot_buckets = L->num_slot_buckets;
+    }
     la.log2s = 0;
     if (a->exact_order == 0 && a->narrow_variant >= 6 && a->dtype != GRG_B200_MIXED) {
         if (a->narrow_split >= 0) {

@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 8
+#define GRG_B200_ABI_VERSION 9
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -119,6 +119,11 @@ typedef enum grg_b200_bias {
  * ring_slot < 0: blob is device memory.  ring_slot >= 0: blob is pinned host memory that
  * grg_b200_traverse copies into ring slot `ring_slot` before the level runs.
  */
+/* Slot layout: the narrow rows form buckets of consecutive positions whose lists all hold the
+ * same number of 4-entry quads, so a kernel computes a row's list from its position
+ * (slot_entry[b] + (p - slot_pos[b]) * 4 * slot_width[b]) instead of loading row_ptr. */
+#define GRG_B200_MAX_SLOT_BUCKETS 8
+
 typedef struct grg_b200_level {
     int64_t row_begin;
     int64_t num_rows;
@@ -133,7 +138,10 @@ typedef struct grg_b200_level {
     int64_t off_row_ids; /* -1: identity order */
     int64_t off_entries;
     int32_t list_align;  /* 1 or 4 */
-    int32_t reserved;
+    int32_t num_slot_buckets; /* 0, or the slot layout of the narrow rows (list_align 4): */
+    int64_t slot_pos[GRG_B200_MAX_SLOT_BUCKETS];   /* first processing position of bucket b */
+    int64_t slot_entry[GRG_B200_MAX_SLOT_BUCKETS]; /* first entry of bucket b */
+    int32_t slot_width[GRG_B200_MAX_SLOT_BUCKETS]; /* entries per row of bucket b, in quads of 4 */
 } grg_b200_level;
 
 typedef struct grg_b200_ring grg_b200_ring; /* opaque: copy stream + per-slot events */

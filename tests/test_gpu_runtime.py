@@ -448,3 +448,34 @@ def test_dataflow_wait_times_out_with_a_status_instead_of_hanging(synth_artifact
         # the context is still usable and the next complete traversal is right
         np.testing.assert_array_equal(grg.matmul(x, "up"), good)
         assert int(runtime._df_sync[2].item()) == 0
+
+
+@pytest.mark.parametrize("variant", [6, 7, 8])
+@pytest.mark.parametrize("exact", [False, True])
+def test_slot_layout_matches_row_pointer_layout(synth_artifact, variant, exact):
+    """Narrow lists located from the slot table (no row_ptr load) give bit-identical results to
+    the row_ptr layout, in both modes, with init values and miss rows."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(900 + variant)
+    k = 8
+    x_up = None
+    results = {}
+    for slots in (False, True):
+        plan = B200Plan(narrow_variant=variant, heavy_threshold=24, exact_order=exact, slots=slots)
+        with _runtime(_layout([synth_artifact], requirements=_req(k=k), pair=B200PlanPair(plan_up=plan, plan_down=plan))) as runtime:
+            (grg,) = runtime.grgs
+            if x_up is None:
+                x_up = rng.standard_normal((k, grg.num_samples))
+                x_dn = rng.standard_normal((k, grg.num_mutations))
+                miss = rng.standard_normal((k, grg.num_mutations))
+                init = rng.standard_normal(k)
+            levels = runtime._artifacts[0].levels
+            assert all((lv.num_slot_buckets > 0) == slots for d in levels for lv in levels[d].array if lv.num_rows > lv.num_heavy)
+            results[slots] = (grg.matmul(x_up, "up", init=init), grg.matmul(x_dn, "down", miss=miss.copy()))
+            assert runtime.device_error() == 0
+    for a, b in zip(results[False], results[True]):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_allclose(results[True][0], oracle.matmul(x_up, "up", init=init), rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(results[True][1], oracle.matmul(x_dn, "down", miss=miss.copy()), rtol=1e-12, atol=1e-9)

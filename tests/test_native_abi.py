@@ -41,6 +41,7 @@ def test_header_constants_match_binding():
     assert define("GRG_B200_SRC_SHIFT") == nat.SRC_SHIFT
     assert define("GRG_B200_ID_MASK") == nat.ID_MASK
     assert define("GRG_B200_NARROW_VARIANTS") == nat.NARROW_VARIANTS
+    assert define("GRG_B200_MAX_SLOT_BUCKETS") == nat.MAX_SLOT_BUCKETS
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")

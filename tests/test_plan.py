@@ -141,19 +141,34 @@ def test_mixed_precision_rejects_incompatible_options():
 
 @pytest.mark.parametrize("heavy", [1, 2, 128])
 @pytest.mark.parametrize("name", ["band3", "overlap4", "synth_haploid", "synth_diploid", "synth_repeat", "sparse_selector"])
-def test_planned_bytes_bound_the_built_level_blobs(name, heavy):
+@pytest.mark.parametrize("slots", [False, True])
+def test_planned_bytes_bound_the_built_level_blobs(name, heavy, slots):
     """Every level blob the runtime builds fits the bytes the planner budgeted for it."""
     from grg_spmv_b200.artifact import iter_artifact_blocks, load_grg_spmv_header
     from grg_spmv_b200.backends.b200.structures import build_down_levels, build_up_levels, load_blocks
 
-    pair = B200PlanPair(plan_up=B200Plan(heavy_threshold=heavy), plan_down=B200Plan(heavy_threshold=heavy))
+    pair = B200PlanPair(plan_up=B200Plan(heavy_threshold=heavy, slots=slots), plan_down=B200Plan(heavy_threshold=heavy, slots=slots))
     layout = _plan((name,), pair=pair)
     st = load_grg_spmv_header(artifact_path(name), np.float64)
     coo = load_blocks(iter_artifact_blocks(artifact_path(name)))
-    up = {lv.level: lv for lv in build_up_levels(st.level_offsets, coo, heavy, False, True, True)}
+    up = {lv.level: lv for lv in build_up_levels(st.level_offsets, coo, heavy, False, True, True, slots=slots)}
     down = {lv.level: lv for lv in build_down_levels(st.level_offsets, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations),
-                                                     (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations), heavy, True, True, True)}
+                                                     (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations), heavy, True, True, True,
+                                                     slots=slots)}
     for lp in layout.artifacts[0].levels_up:
         assert up[lp.level].layout()[4] <= lp.nbytes
     for lp in layout.artifacts[0].levels_down:
         assert down[lp.level].layout()[4] <= lp.nbytes
+    for lv in list(up.values()) + list(down.values()):
+        if not slots:
+            assert lv.slots is None
+            continue
+        # the slot table locates every narrow list exactly where row_ptr does
+        narrow = lv.num_rows - lv.heavy_rows.size
+        assert lv.slots is not None and lv.slots.shape[0] <= 8
+        bounds = list(lv.slots[:, 0]) + [narrow]
+        for b, (pos0, entry0, width) in enumerate(lv.slots):
+            pos = np.arange(pos0, bounds[b + 1])
+            np.testing.assert_array_equal(lv.row_ptr[pos], entry0 + (pos - pos0) * 4 * width)
+            np.testing.assert_array_equal(lv.row_ptr[pos + 1] - lv.row_ptr[pos], 4 * width)
+            assert b == 0 or width < lv.slots[b - 1, 2]  # longest bucket first
