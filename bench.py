@@ -56,6 +56,7 @@ def parse_args():
     p.add_argument("--exact-order", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--e2e-inflight", type=int, default=2, help="end-to-end steps in flight (one runtime and stream each)")
     p.add_argument("--no-tiers", action="store_true",
                    help="skip the batched / mixed-precision comparison on uneven RHS blocks (runs at N=1 only)")
     p.add_argument("--tier-blocks", default="1,3,16,64,256", help="RHS block widths of the tier comparison")
@@ -74,6 +75,7 @@ def parse_args():
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
     p.add_argument("--slots", action="store_true", help="pad narrow rows to their bucket width (list offset from position)")
+    p.add_argument("--pdl", action="store_true", help="launch level kernels with programmatic dependent launch")
     p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
     p.add_argument("--schedule", choices=["levels", "dataflow"], default=None,
                    help="one launch per level, or one persistent dataflow launch per traversal")
@@ -245,6 +247,8 @@ def run_b200(args) -> None:
         extra["long_first"] = False
     if args.slots:
         extra["slots"] = True
+    if args.pdl:
+        extra["pdl"] = True
     if args.narrow_split is not None:
         extra["narrow_split"] = args.narrow_split
     if args.schedule is not None:
@@ -375,38 +379,67 @@ def run_b200(args) -> None:
     peak, peak_kind = measured_peak_hbm()
     achieved = lv_bytes / (level_total_ms / 1e3) / 1e9
 
-    # End-to-end through the public API with pinned host buffers.
+    # End-to-end through the public API with pinned host buffers: every step copies its input
+    # and miss rows in and both outputs out.  Two steps are in flight, each on its own runtime
+    # and stream (``--e2e-inflight``), so one step's copies overlap the other's kernels.
     e2e = None
     if not args.no_e2e:
+        lanes = [(stream, runtime, up, down)]
+        extra_runtimes = []
+        for _ in range(max(args.e2e_inflight, 1) - 1):
+            s2 = torch.cuda.Stream(device=device)
+            lay2 = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0,
+                                    ring_buffer_size=0, device=local_rank, stream=s2, pair=pair, precision=args.precision)
+            rt2 = B200Runtime(lay2, use_graphs=not args.no_graphs).__enter__()
+            extra_runtimes.append(rt2)
+            (g2,) = rt2.grgs
+            with torch.cuda.device(device), torch.cuda.stream(s2):
+                lanes.append((s2, rt2, g2.prepare_matmul_cuda(direction="up", k=k),
+                              g2.prepare_matmul_cuda(direction="down", k=k, use_miss=True)))
         x_host = torch.from_numpy(x_up_np).pin_memory()
         miss_host = torch.from_numpy(miss_np).pin_memory()
-        out_up_host = torch.empty((k, M), dtype=torch.float64).pin_memory()
-        out_down_host = torch.empty((k, S), dtype=torch.float64).pin_memory()
-        with torch.cuda.device(device), torch.cuda.stream(stream):
-            def e2e_step():
-                up.input.copy_(x_host, non_blocking=True)
-                up()
-                out_up_host.copy_(up.output, non_blocking=True)
-                down.miss_input.copy_(miss_host, non_blocking=True)
-                down()
-                out_down_host.copy_(down.output, non_blocking=True)
+        outs = [(torch.empty((k, M), dtype=torch.float64).pin_memory(), torch.empty((k, S), dtype=torch.float64).pin_memory())
+                for _ in lanes]
 
-            for _ in range(max(args.warmup, 1)):
-                e2e_step()
+        def e2e_step(i: int) -> None:
+            st, _, op_up, op_down = lanes[i % len(lanes)]
+            out_up_host, out_down_host = outs[i % len(lanes)]
+            with torch.cuda.stream(st):
+                op_up.input.copy_(x_host, non_blocking=True)
+                op_up()
+                out_up_host.copy_(op_up.output, non_blocking=True)
+                op_down.miss_input.copy_(miss_host, non_blocking=True)
+                op_down()
+                out_down_host.copy_(op_down.output, non_blocking=True)
+
+        with torch.cuda.device(device):
+            for i in range(max(args.warmup, 1) * len(lanes)):
+                e2e_step(i)
             synced_barrier()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
-            for _ in range(args.steps):
-                e2e_step()
+            for st, *_ in lanes[1:]:
+                st.wait_stream(stream)
+            for i in range(args.steps):
+                e2e_step(i)
+            for st, *_ in lanes[1:]:
+                stream.wait_stream(st)
             b.record(stream)
             synced_barrier()
             e2e_ms = a.elapsed_time(b)
+        # every lane computed the same step: their host outputs must agree bit for bit
+        lanes_agree = all(np.array_equal(o[0].numpy(), outs[0][0].numpy()) and np.array_equal(o[1].numpy(), outs[0][1].numpy())
+                          for o in outs[1:])
+        for rt2 in extra_runtimes:
+            rt2.__exit__(None, None, None)
+        del extra_runtimes, lanes
         if world > 1:
             t = torch.tensor([e2e_ms], device=device, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_ms = float(t[0])
         e2e = {"value": total_work / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms / args.steps,
-               "h2d_bytes_per_step": int((S + M) * k * 8), "d2h_bytes_per_step": int((M + S) * k * 8)}
+               "h2d_bytes_per_step": int((S + M) * k * 8), "d2h_bytes_per_step": int((M + S) * k * 8),
+               "steps_in_flight": max(args.e2e_inflight, 1), "lanes_agree": bool(lanes_agree)}
 
     # CPU baseline (oracle) and a parity spot check of the same step, rank 0 at N=1.
     cpu = None
@@ -449,6 +482,9 @@ def run_b200(args) -> None:
             gen_multi = time.perf_counter() - t0
             tiers["multi_graph"] = measure_tiers(args, multi, device, stream)
             tiers["multi_graph"]["generate_s"] = gen_multi
+            torch.cuda.empty_cache()
+            # many narrow blocks: where merging blocks and overlapping graphs pay most
+            tiers["multi_graph_small_blocks"] = measure_tiers(args, multi, device, stream, blocks=[1, 1, 2, 3, 3, 4])
     traffic, traffic_src = profiled_traffic(E, k, args.precision, pair.plan_down.schedule)
     if rank == 0:
         line = {
@@ -470,7 +506,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "slots": pair.plan_down.slots, "narrow_split": pair.plan_down.narrow_split,
+                       "long_first": pair.plan_down.long_first, "slots": pair.plan_down.slots, "pdl": pair.plan_down.pdl, "narrow_split": pair.plan_down.narrow_split,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
@@ -526,7 +562,7 @@ def make_multi_artifacts(args) -> list[Path]:
     return paths
 
 
-def measure_tiers(args, paths, device, stream) -> dict:
+def measure_tiers(args, paths, device, stream, blocks=None) -> dict:
     """Uneven RHS blocks on every graph of ``paths``, three ways, same work (sum of blocks, up
     and down, every graph): the plain FP64 drop-in (one prepared op per block, direction and
     graph, one after another), a plain FP64 batch (one CUDA graph: blocks of a graph merged and
@@ -538,7 +574,7 @@ def measure_tiers(args, paths, device, stream) -> dict:
     from grg_spmv_b200 import RuntimeRequirements
     from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
 
-    blocks = [int(b) for b in args.tier_blocks.split(",") if b]
+    blocks = blocks or [int(b) for b in args.tier_blocks.split(",") if b]
     kmax = max(blocks)
     req = RuntimeRequirements(max_k_up=kmax, max_k_down=kmax, need_down_miss_input=True, need_up_miss_output=False,
                               need_init_vector=False, need_init_matrix=False, need_init_xtx=False)

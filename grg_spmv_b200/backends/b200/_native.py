@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 9
+ABI_VERSION = 10
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -29,6 +29,7 @@ NVCC_FLAGS = (
 OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED = 0, 1, 2, 3
 F64, F32, MIXED = 0, 1, 2
 MAX_SLOT_BUCKETS = 8
+LAUNCH_PDL = 1
 SCHEDULE_LEVELS, SCHEDULE_DATAFLOW = 0, 1
 DEVICE_WAIT_TIMEOUT = 6
 UP, DOWN = 0, 1
@@ -133,6 +134,8 @@ class TraverseArgs(ctypes.Structure):
         ("narrow_split", ctypes.c_int32),
         ("schedule", ctypes.c_int32),
         ("dataflow_sync", ctypes.c_void_p),
+        ("launch_flags", ctypes.c_int32),
+        ("reserved3", ctypes.c_int32),
     ]
 
 

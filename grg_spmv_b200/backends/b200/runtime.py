@@ -494,6 +494,7 @@ class B200Runtime:
             heavy = 2 if a.narrow_variant >= 6 else (1 if k <= 16 else 0)
         a.heavy_variant = int(heavy)
         a.narrow_split = int(plan.narrow_split)
+        a.launch_flags = nat.LAUNCH_PDL if plan.pdl else 0
         a.schedule = nat.SCHEDULE_DATAFLOW if plan.schedule == "dataflow" else nat.SCHEDULE_LEVELS
         a.dataflow_sync = _ptr(self._df_sync if df_sync is None else df_sync)
         return a

@@ -60,6 +60,23 @@ int fail(int code, const char* fmt, ...) {
             return fail(GRG_B200_ERR_CUDA, "launch of %s failed: %s", name, cudaGetErrorString(err__)); \
     } while (0)
 
+// Launch with programmatic dependent launch when `pdl` (the kernel must call pdl_wait()
+// before touching data that earlier kernels of the stream produce).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(bool pdl, cudaStream_t s, dim3 grid, int block, void (*kernel)(KArgs...), Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(static_cast<unsigned>(block));
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? attr : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // ---------------------------------------------------------------------------------------
 // Vector packs
 // ---------------------------------------------------------------------------------------
@@ -179,6 +196,14 @@ enum DeviceError : int32_t {
 __device__ __forceinline__ void report(int32_t* err, int32_t code) {
     if (err) atomicCAS(err, 0, code);
 }
+
+// Programmatic dependent launch: a kernel launched with it may start while the previous
+// kernel of the stream is finishing; it reads only static data (level lists) until
+// pdl_wait(), which returns once the previous grid has completed and its writes are visible
+// (immediately when the launch did not use the attribute).  pdl_trigger() lets the next
+// kernel launch once every CTA of this grid has started.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 template <typename T, int V, int INIT>
 __device__ __forceinline__ Pack<T, V> init_value(const LevelArgs& a, int64_t row, int64_t c) {
@@ -441,6 +466,10 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
     const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
     const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    uint4 first[Q];  // the list is static: fetched before waiting for the previous level
+#pragma unroll
+    for (int j = 0; j < Q; ++j) first[j] = (e0 >> 2) + j < (e1 >> 2) ? __ldg(codes4 + (e0 >> 2) + j) : null4;
+    pdl_wait();
     T* state = static_cast<T*>(a.state);
     const int64_t step = static_cast<int64_t>(V) << a.log2g;
     for (int64_t c = static_cast<int64_t>(glane) * V; c < a.k; c += step) {
@@ -450,7 +479,7 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
         int32_t q = e0 >> 2;
         uint4 cur[Q];
 #pragma unroll
-        for (int j = 0; j < Q; ++j) cur[j] = q + j < q1 ? __ldg(codes4 + q + j) : null4;
+        for (int j = 0; j < Q; ++j) cur[j] = first[j];
         for (; q < q1; q += Q) {  // Q quads (4 * Q row fetches) in flight per round
             uint4 nxt[Q];
 #pragma unroll
@@ -514,6 +543,7 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
         e1 = __ldg(a.row_ptr + pos + 1);
         row = level_row(a, pos);
     }
+    pdl_wait();
     const int glane = lane & ((1 << a.log2g) - 1);
     const int sub = (lane >> a.log2g) & ((1 << a.log2s) - 1);
     const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
@@ -552,6 +582,7 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
 // quads, eight row fetches, in flight per round).
 template <typename T, int V, int INIT, int MB, int Q = 1>
 __global__ void __launch_bounds__(kNarrowThreads, MB) level_vec_kernel(LevelArgs a) {
+    pdl_trigger();
     vec_rows<T, V, INIT, Q>(a, blockIdx.x);
 }
 
@@ -572,6 +603,7 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
     const int32_t e0 = __ldg(a.row_ptr + pos);
     const int32_t e1 = __ldg(a.row_ptr + pos + 1);
     const int64_t row = level_row(a, pos);
+    pdl_wait();
     const int g_lanes = 1 << a.log2g;
     const int groups = 32 >> a.log2g;
     const int glane = lane32 & (g_lanes - 1);
@@ -626,6 +658,7 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
 
 template <typename T, int V, int INIT>
 __global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a) {
+    pdl_trigger();
     warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
 }
 
@@ -637,6 +670,7 @@ __global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a
 template <typename T, int V, int INIT, bool SPLIT, int MB, int Q = 1>
 __global__ void __launch_bounds__(kNarrowThreads, MB) level_fused_kernel(LevelArgs a, int64_t heavy_blocks) {
     static_assert(kNarrowThreads == kWarpRowThreads, "both row kinds use the same CTA shape");
+    pdl_trigger();
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
     else if constexpr (SPLIT) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
     else vec_rows<T, V, INIT, Q>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
@@ -1344,6 +1378,7 @@ __global__ void __launch_bounds__(256) sentinel_fill_kernel(T* state, int64_t n)
 // Up seeding of level 0: state[r] = init(r) (+ input row for samples).
 template <typename T, int V, int INIT>
 __global__ void __launch_bounds__(256) seed_up_kernel(LevelArgs a, int64_t num_samples, const int32_t* s2i, int32_t by_ind) {
+    pdl_trigger();
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t row = t >> a.log2g;
     if (row >= a.num_rows) return;
@@ -1357,6 +1392,7 @@ __global__ void __launch_bounds__(256) seed_up_kernel(LevelArgs a, int64_t num_s
             return;
         }
     }
+    pdl_wait();  // inputs, init values and the state it overwrites belong to earlier kernels
     const int64_t step = static_cast<int64_t>(V) << a.log2g;
     for (int64_t c = static_cast<int64_t>(lane) * V; c < a.k; c += step) {
         Pack<T, V> v = init_value<T, V, INIT>(a, row, c);
@@ -1400,6 +1436,7 @@ __device__ __forceinline__ void apply_bias(const OutArgs& a, int64_t r, int64_t 
 // out[r] = sum over idx[ptr[r]..ptr[r+1]) of state rows (from zero, in order) + bias.
 template <typename T, int V, bool BIAS_PER_ENTRY>
 __global__ void __launch_bounds__(256) gather_out_kernel(OutArgs a) {
+    pdl_wait();
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t r = t >> a.log2g;
     if (r >= a.rows) return;
@@ -1428,6 +1465,7 @@ __global__ void __launch_bounds__(256) gather_out_kernel(OutArgs a) {
 // Down output without grouping: out[s] = state[s] + bias[s].
 template <typename T, int V>
 __global__ void __launch_bounds__(256) copy_out_kernel(OutArgs a) {
+    pdl_wait();
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t r = t >> a.log2g;
     if (r >= a.rows) return;
@@ -1445,6 +1483,7 @@ __global__ void __launch_bounds__(256) copy_out_kernel(OutArgs a) {
 // All nodes in original order: out[j] = state[inv_perm[j]].
 template <typename T, int V>
 __global__ void __launch_bounds__(256) emit_all_kernel(OutArgs a) {
+    pdl_wait();
     const int64_t t = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     const int64_t j = t >> a.log2g;
     if (j >= a.rows) return;
@@ -1651,7 +1690,7 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
 }
 
 template <typename T, int V>
-int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, cudaStream_t s) {
+int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, bool pdl, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     const bool padded_variant = variant >= 6 && variant <= 8;
     if (padded_variant && heavy_variant == 2 && !exact) {
@@ -1661,12 +1700,12 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
 #define GRG_FUSED_MB(INIT, MB)                                                                                 \
-    if (la.log2s > 0) level_fused_kernel<T, V, INIT, true, MB><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); \
-    else level_fused_kernel<T, V, INIT, false, MB><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks);
+    if (la.log2s > 0) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, true, MB>, la, heavy_blocks)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, false, MB>, la, heavy_blocks));
 #define GRG_FUSED(INIT)                                                                                  \
     if (variant == 8) {                                                                                  \
-        if (la.log2s > 0) level_fused_kernel<T, V, INIT, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks); \
-        else level_fused_kernel<T, V, INIT, false, 3, 2><<<grid, kNarrowThreads, 0, s>>>(la, heavy_blocks);          \
+        if (la.log2s > 0) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, true, 6>, la, heavy_blocks)); \
+        else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, false, 3, 2>, la, heavy_blocks));          \
     } else if (variant == 7) {                                                                           \
         GRG_FUSED_MB(INIT, 5)                                                                            \
     } else {                                                                                             \
@@ -1688,10 +1727,10 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
         switch (init_mode) {
-            case 0: level_fused_kernel<T, V, 0, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
-            case 1: level_fused_kernel<T, V, 1, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
-            case 2: level_fused_kernel<T, V, 2, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
-            default: level_fused_kernel<T, V, 3, true, 6><<<grid, kNarrowThreads, 0, s>>>(la, 0); break;
+            case 0: GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, 0, true, 6>, la, 0)); break;
+            case 1: GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, 1, true, 6>, la, 0)); break;
+            case 2: GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, 2, true, 6>, la, 0)); break;
+            default: GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, 3, true, 6>, la, 0)); break;
         }
         GRG_LAUNCH_CHECK("level_fused_kernel(split)");
     } else if (narrow > 0 && padded_variant) {
@@ -1699,9 +1738,9 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
 #define GRG_VEC(INIT)                                                                      \
-    if (variant == 8) level_vec_kernel<T, V, INIT, 3, 2><<<grid, kNarrowThreads, 0, s>>>(la); \
-    else if (variant == 7) level_vec_kernel<T, V, INIT, 5><<<grid, kNarrowThreads, 0, s>>>(la); \
-    else level_vec_kernel<T, V, INIT, 6><<<grid, kNarrowThreads, 0, s>>>(la);
+    if (variant == 8) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 3, 2>, la)); \
+    else if (variant == 7) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 5>, la)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 6>, la));
         switch (init_mode) {
             case 0: GRG_VEC(0) break;
             case 1: GRG_VEC(1) break;
@@ -1746,10 +1785,10 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
         switch (init_mode) {
-            case 0: level_warp_kernel<T, V, 0><<<grid, kWarpRowThreads, 0, s>>>(la); break;
-            case 1: level_warp_kernel<T, V, 1><<<grid, kWarpRowThreads, 0, s>>>(la); break;
-            case 2: level_warp_kernel<T, V, 2><<<grid, kWarpRowThreads, 0, s>>>(la); break;
-            default: level_warp_kernel<T, V, 3><<<grid, kWarpRowThreads, 0, s>>>(la); break;
+            case 0: GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_warp_kernel<T, V, 0>, la)); break;
+            case 1: GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_warp_kernel<T, V, 1>, la)); break;
+            case 2: GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_warp_kernel<T, V, 2>, la)); break;
+            default: GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_warp_kernel<T, V, 3>, la)); break;
         }
         GRG_LAUNCH_CHECK("level_warp_kernel");
     } else if (la.num_heavy > 0) {
@@ -1874,11 +1913,13 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     const bool exact = a->exact_order != 0;
     if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, a->narrow_variant, s);
     return dispatch(a, sh, [&](auto t, auto v) {
-        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant, s);
+        return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant,
+                                                                   (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0, s);
     });
 }
 
 int seed_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    const bool pdl = (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0;
     if (a->level0_rows <= 0) return GRG_B200_OK;
     if (!a->input) return fail(GRG_B200_ERR_INVALID, "input is NULL");
     if (a->by_individual && !a->sample_to_individual) return fail(GRG_B200_ERR_INVALID, "sample_to_individual is NULL");
@@ -1900,10 +1941,10 @@ int seed_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t 
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
         switch (a->init_mode) {
-            case 0: seed_up_kernel<T, V, 0><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
-            case 1: seed_up_kernel<T, V, 1><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
-            case 2: seed_up_kernel<T, V, 2><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
-            default: seed_up_kernel<T, V, 3><<<grid, 256, 0, s>>>(la, a->num_samples, a->sample_to_individual, a->by_individual); break;
+            case 0: GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, seed_up_kernel<T, V, 0>, la, a->num_samples, a->sample_to_individual, a->by_individual)); break;
+            case 1: GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, seed_up_kernel<T, V, 1>, la, a->num_samples, a->sample_to_individual, a->by_individual)); break;
+            case 2: GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, seed_up_kernel<T, V, 2>, la, a->num_samples, a->sample_to_individual, a->by_individual)); break;
+            default: GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, seed_up_kernel<T, V, 3>, la, a->num_samples, a->sample_to_individual, a->by_individual)); break;
         }
         GRG_LAUNCH_CHECK("seed_up_kernel");
         return (int)GRG_B200_OK;
@@ -1929,6 +1970,7 @@ OutArgs out_args(const grg_b200_traverse_args* a, const Shape& sh) {
 }
 
 int output_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    const bool pdl = (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0;
     if (!a->output || !a->sel_mut_ptr || (!a->sel_mut_idx && a->num_mutations > 0))
         return fail(GRG_B200_ERR_INVALID, "up output needs output and sel_mut");
     if (a->use_miss && (!a->miss || !a->sel_miss_ptr)) return fail(GRG_B200_ERR_INVALID, "up miss output needs miss and sel_miss");
@@ -1956,7 +1998,7 @@ int output_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
-        gather_out_kernel<T, V, false><<<grid, 256, 0, s>>>(o);
+        GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, gather_out_kernel<T, V, false>, o));
         GRG_LAUNCH_CHECK("gather_out_kernel(sel_mut)");
         if (a->use_miss) {
             OutArgs m = o;
@@ -1965,7 +2007,7 @@ int output_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_
             m.out = a->miss;
             m.ld_out = a->ld_miss;
             m.bias_mode = GRG_B200_BIAS_NONE;
-            gather_out_kernel<T, V, false><<<grid, 256, 0, s>>>(m);
+            GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, gather_out_kernel<T, V, false>, m));
             GRG_LAUNCH_CHECK("gather_out_kernel(sel_miss)");
         }
         return (int)GRG_B200_OK;
@@ -1973,6 +2015,7 @@ int output_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_
 }
 
 int output_down_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    const bool pdl = (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0;
     if (!a->output) return fail(GRG_B200_ERR_INVALID, "output is NULL");
     OutArgs o = out_args(a, sh);
     if (a->by_individual) {
@@ -1995,14 +2038,15 @@ int output_down_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStrea
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
-        if (a->by_individual) gather_out_kernel<T, V, true><<<grid, 256, 0, s>>>(o);
-        else copy_out_kernel<T, V><<<grid, 256, 0, s>>>(o);
+        if (a->by_individual) GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, gather_out_kernel<T, V, true>, o));
+        else GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, copy_out_kernel<T, V>, o));
         GRG_LAUNCH_CHECK("output_down");
         return (int)GRG_B200_OK;
     });
 }
 
 int emit_all_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
+    const bool pdl = (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0;
     if (!a->output || !a->inv_node_perm) return fail(GRG_B200_ERR_INVALID, "emit_all_nodes needs output and inv_node_perm");
     OutArgs o = out_args(a, sh);
     o.rows = a->num_nodes;
@@ -2016,7 +2060,7 @@ int emit_all_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t
     return dispatch(a, sh, [&](auto t, auto v) {
         using T = decltype(t);
         constexpr int V = decltype(v)::value;
-        emit_all_kernel<T, V><<<grid, 256, 0, s>>>(o);
+        GRG_CUDA_TRY(launch_k(pdl, s, grid, 256, emit_all_kernel<T, V>, o));
         GRG_LAUNCH_CHECK("emit_all_kernel");
         return (int)GRG_B200_OK;
     });
@@ -2258,6 +2302,12 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
         if (a->emit_all_nodes) return emit_all_impl(a, sh, s);
         if (a->direction == GRG_B200_UP) return output_up_impl(a, sh, s);
         return output_down_impl(a, sh, s);
+    }
+    grg_b200_traverse_args no_pdl;
+    if (any_streamed && (a->launch_flags & GRG_B200_LAUNCH_PDL)) {  // ring copies sit between the level launches
+        no_pdl = *a;
+        no_pdl.launch_flags &= ~GRG_B200_LAUNCH_PDL;
+        a = &no_pdl;
     }
     if (a->direction == GRG_B200_UP) {
         rc = seed_up_impl(a, sh, s);

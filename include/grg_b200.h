@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 9
+#define GRG_B200_ABI_VERSION 10
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -217,7 +217,15 @@ typedef struct grg_b200_traverse_args {
     int32_t schedule;                   /* grg_b200_schedule */
     void* dataflow_sync;                /* GRG_B200_SCHEDULE_DATAFLOW: device int32[4], 16-byte aligned;
                                            [2] holds GRG_B200_DEVICE_WAIT_TIMEOUT after a failed wait */
+    int32_t launch_flags;               /* GRG_B200_LAUNCH_* bits */
+    int32_t reserved3;
 } grg_b200_traverse_args;
+
+/* Level, seed and output launches of the default kernels use programmatic dependent launch:
+ * each may start while the previous kernel of the stream finishes, reads only the static
+ * level lists until the hardware reports that kernel complete, and so overlaps the launch
+ * gap.  Ignored when any level is streamed. */
+#define GRG_B200_LAUNCH_PDL 1
 
 /*
  * GRG_B200_SCHEDULE_LEVELS: one launch per level (each level waits for the previous one).

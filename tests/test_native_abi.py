@@ -42,6 +42,8 @@ def test_header_constants_match_binding():
     assert define("GRG_B200_ID_MASK") == nat.ID_MASK
     assert define("GRG_B200_NARROW_VARIANTS") == nat.NARROW_VARIANTS
     assert define("GRG_B200_MAX_SLOT_BUCKETS") == nat.MAX_SLOT_BUCKETS
+    assert define("GRG_B200_LAUNCH_PDL") == nat.LAUNCH_PDL
+    assert define("GRG_B200_DEVICE_WAIT_TIMEOUT") == nat.DEVICE_WAIT_TIMEOUT
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
