@@ -474,17 +474,18 @@ def run_b200(args) -> None:
     torch.cuda.empty_cache()
     tiers = None
     if world == 1 and not args.no_tiers:
-        tiers = {"single_graph": measure_tiers(args, [path], device, stream)}
+        config_blocks = [int(b) for b in args.tier_blocks.split(",") if b]
+        tiers = {"single_graph": measure_tiers(args, [path], device, stream, [config_blocks])[0]}
         torch.cuda.empty_cache()
         if args.tier_grgs > 0:
             t0 = time.perf_counter()
             multi = make_multi_artifacts(args)
             gen_multi = time.perf_counter() - t0
-            tiers["multi_graph"] = measure_tiers(args, multi, device, stream)
+            # the configuration's blocks, then many narrow blocks (where merging blocks and
+            # overlapping graphs pay most)
+            tiers["multi_graph"], tiers["multi_graph_small_blocks"] = measure_tiers(
+                args, multi, device, stream, [config_blocks, [1, 1, 2, 3, 3, 4]])
             tiers["multi_graph"]["generate_s"] = gen_multi
-            torch.cuda.empty_cache()
-            # many narrow blocks: where merging blocks and overlapping graphs pay most
-            tiers["multi_graph_small_blocks"] = measure_tiers(args, multi, device, stream, blocks=[1, 1, 2, 3, 3, 4])
     traffic, traffic_src = profiled_traffic(E, k, args.precision, pair.plan_down.schedule)
     if rank == 0:
         line = {
@@ -562,41 +563,29 @@ def make_multi_artifacts(args) -> list[Path]:
     return paths
 
 
-def measure_tiers(args, paths, device, stream, blocks=None) -> dict:
+def measure_tiers(args, paths, device, stream, block_sets) -> list[dict]:
     """Uneven RHS blocks on every graph of ``paths``, three ways, same work (sum of blocks, up
     and down, every graph): the plain FP64 drop-in (one prepared op per block, direction and
     graph, one after another), a plain FP64 batch (one CUDA graph: blocks of a graph merged and
     tiled, graphs on concurrent streams, autotuned) and a mixed-precision batch.  Device time
     with CUDA events; errors of each batch against the FP64 drop-in's outputs and, for the
-    blocks of width <= 3 on the first graph, against the CPU oracle."""
+    blocks of width <= 3 on the first graph, against the CPU oracle.  One result per block set
+    of ``block_sets``, all on one runtime."""
     import torch
 
     from grg_spmv_b200 import RuntimeRequirements
     from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
 
-    blocks = blocks or [int(b) for b in args.tier_blocks.split(",") if b]
-    kmax = max(blocks)
+    kmax = max(max(b) for b in block_sets)
     req = RuntimeRequirements(max_k_up=kmax, max_k_down=kmax, need_down_miss_input=True, need_up_miss_output=False,
                               need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
     layout = plan_b200_layout(artifacts=[str(p) for p in paths], dtype=np.float64, requirements=req, vram_budget_bytes=0,
                               ring_buffer_size=0, device=device.index or 0, stream=stream)
     rng = np.random.default_rng(7)
     rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(float(np.max(np.abs(ref))), 1e-300))
-    out = {"blocks": blocks, "steps": args.tier_steps, "warmup": max(args.warmup, 3)}
+    oracle = None
+    results = []
     with B200Runtime(layout) as rt, torch.cuda.device(device), torch.cuda.stream(stream):
-        items = []
-        for g in rt.grgs:
-            items += [(g, "up", kb) for kb in blocks] + [(g, "down", kb, True) for kb in blocks]
-        xs, misses = [], []
-        for it in items:
-            g = it[0]
-            cols = g.num_samples if it[1] == "up" else g.num_mutations
-            xs.append(torch.from_numpy(rng.standard_normal((it[2], cols))).to(device))
-            misses.append(torch.from_numpy(rng.standard_normal((it[2], g.num_mutations))).to(device) if it[1] == "down" else None)
-        work = 2.0 * sum(g.num_edges for g in rt.grgs) * sum(blocks)
-        out["graphs"] = [{"num_edges": g.num_edges, "num_nodes": g.num_nodes, "num_mutations": g.num_mutations}
-                         for g in rt.grgs]
-
         def timed(step) -> float:
             for _ in range(max(args.warmup, 3)):
                 step()
@@ -609,59 +598,76 @@ def measure_tiers(args, paths, device, stream, blocks=None) -> dict:
             torch.cuda.synchronize(device)
             return a.elapsed_time(b) / args.tier_steps
 
-        # 1) plain FP64 drop-in: one prepared op per block and direction.
-        ops = [it[0].prepare_matmul_cuda(direction=it[1], k=it[2], use_miss=it[1] == "down") for it in items]
-        plain_out = [None] * len(items)
+        for blocks in block_sets:
+            out = {"blocks": list(blocks), "steps": args.tier_steps, "warmup": max(args.warmup, 3)}
+            items = []
+            for g in rt.grgs:
+                items += [(g, "up", kb) for kb in blocks] + [(g, "down", kb, True) for kb in blocks]
+            xs, misses = [], []
+            for it in items:
+                g = it[0]
+                cols = g.num_samples if it[1] == "up" else g.num_mutations
+                xs.append(torch.from_numpy(rng.standard_normal((it[2], cols))).to(device))
+                misses.append(torch.from_numpy(rng.standard_normal((it[2], g.num_mutations))).to(device) if it[1] == "down" else None)
+            work = 2.0 * sum(g.num_edges for g in rt.grgs) * sum(blocks)
+            out["graphs"] = [{"num_edges": g.num_edges, "num_nodes": g.num_nodes, "num_mutations": g.num_mutations}
+                             for g in rt.grgs]
+            # 1) plain FP64 drop-in: one prepared op per block and direction.
+            ops = [it[0].prepare_matmul_cuda(direction=it[1], k=it[2], use_miss=it[1] == "down") for it in items]
+            plain_out = [None] * len(items)
 
-        def dropin_step(keep=False):
-            for i, op in enumerate(ops):
-                op.input.copy_(xs[i])
-                if misses[i] is not None:
-                    op.miss_input.copy_(misses[i])
-                op()
-                if keep:
-                    plain_out[i] = op.output.cpu().numpy()
+            def dropin_step(keep=False):
+                for i, op in enumerate(ops):
+                    op.input.copy_(xs[i])
+                    if misses[i] is not None:
+                        op.miss_input.copy_(misses[i])
+                    op()
+                    if keep:
+                        plain_out[i] = op.output.cpu().numpy()
 
-        ms = timed(dropin_step)
-        dropin_step(keep=True)
-        out["plain_f64_dropin"] = {"value": work / (ms / 1e3), "ms_per_step": ms, "launch": "one prepared op per block"}
-        del ops
-        # 2) and 3) batches.
-        for name, precision in (("plain_f64_batched", "plain"), ("mixed_batched", "mixed")):
-            with rt.prepare_batch(items, precision=precision, autotune=True) as batch:
-                def batch_step():
-                    for i in range(len(items)):
-                        batch.inputs[i].copy_(xs[i])
-                        if misses[i] is not None:
-                            batch.miss_inputs[i].copy_(misses[i])
-                    batch()
-
-                ms_b = timed(batch_step)
-                batch_step()
-                torch.cuda.synchronize(device)
-                errs = [rel(batch.outputs[i].cpu().numpy(), plain_out[i]) for i in range(len(items))]
-                out[name] = {"value": work / (ms_b / 1e3), "ms_per_step": ms_b, "tile_k": batch.tile_k,
-                             "tiles": batch.num_tiles, "tuned_ms": {str(k): v for k, v in batch.tuned_ms.items()},
-                             "max_rel_err_vs_plain_f64": max(errs), "speedup_vs_dropin": ms / ms_b}
-                small = [i for i, it in enumerate(items) if it[2] <= 3 and it[0] is rt.grgs[0]]
-                if small and not args.no_cpu_baseline:
+            ms = timed(dropin_step)
+            dropin_step(keep=True)
+            out["plain_f64_dropin"] = {"value": work / (ms / 1e3), "ms_per_step": ms, "launch": "one prepared op per block"}
+            del ops
+            small = [i for i, it in enumerate(items) if it[2] <= 3 and it[0] is rt.grgs[0]]
+            refs = {}
+            if small and not args.no_cpu_baseline:
+                if oracle is None:
                     sys.path.insert(0, str(REPO / "oracle"))
                     from grg_oracle import OracleGRG
 
                     oracle = OracleGRG(paths[0])
-                    oerr, perr = [], []
-                    for i in small:
-                        x_np = xs[i].cpu().numpy()
-                        m_np = misses[i].cpu().numpy() if misses[i] is not None else None
-                        ref = oracle.matmul(x_np, items[i][1], miss=m_np)
-                        oerr.append(rel(batch.outputs[i].cpu().numpy(), ref))
-                        perr.append(rel(plain_out[i], ref))
-                    out[name]["max_rel_err_vs_oracle_blocks_le3"] = max(oerr)
-                    out["plain_f64_dropin"]["max_rel_err_vs_oracle_blocks_le3"] = max(perr)
+                for i in small:
+                    m_np = misses[i].cpu().numpy() if misses[i] is not None else None
+                    refs[i] = oracle.matmul(xs[i].cpu().numpy(), items[i][1], miss=m_np)
+                out["plain_f64_dropin"]["max_rel_err_vs_oracle_blocks_le3"] = max(rel(plain_out[i], refs[i]) for i in refs)
+            # 2) and 3) batches.
+            for name, precision in (("plain_f64_batched", "plain"), ("mixed_batched", "mixed")):
+                with rt.prepare_batch(items, precision=precision, autotune=True) as batch:
+                    def batch_step():
+                        for i in range(len(items)):
+                            batch.inputs[i].copy_(xs[i])
+                            if misses[i] is not None:
+                                batch.miss_inputs[i].copy_(misses[i])
+                        batch()
+
+                    ms_b = timed(batch_step)
+                    batch_step()
+                    torch.cuda.synchronize(device)
+                    errs = [rel(batch.outputs[i].cpu().numpy(), plain_out[i]) for i in range(len(items))]
+                    out[name] = {"value": work / (ms_b / 1e3), "ms_per_step": ms_b, "tile_k": batch.tile_k,
+                                 "tiles": batch.num_tiles, "tuned_ms": {str(k): v for k, v in batch.tuned_ms.items()},
+                                 "max_rel_err_vs_plain_f64": max(errs), "speedup_vs_dropin": ms / ms_b}
+                    if refs:
+                        out[name]["max_rel_err_vs_oracle_blocks_le3"] = max(rel(batch.outputs[i].cpu().numpy(), refs[i])
+                                                                            for i in refs)
+                torch.cuda.empty_cache()
+            out["workload"] = (f"{len(paths)} graph(s); RHS blocks {list(blocks)} in both directions on each (down with "
+                               f"miss rows), inputs copied into the op/batch buffers every step")
+            results.append(out)
+            del xs, misses, plain_out
             torch.cuda.empty_cache()
-    out["workload"] = (f"{len(paths)} graph(s); RHS blocks {blocks} in both directions on each (down with miss "
-                       f"rows), inputs copied into the op/batch buffers every step")
-    return out
+    return results
 
 
 _WORKER_ORACLE = None
