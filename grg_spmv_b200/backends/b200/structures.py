@@ -115,6 +115,14 @@ def canonical_coo(indices: np.ndarray, indptr: np.ndarray, shape) -> tuple[np.nd
     return rows, cols
 
 
+def _bit_length(counts: np.ndarray) -> np.ndarray:
+    """ceil(log2(c + 1)) of non-negative integers, exactly: the number of powers of two <= c."""
+    return np.searchsorted(_POW2, np.asarray(counts, dtype=np.int64), side="right").astype(np.int64)
+
+
+_POW2 = np.asarray([1 << i for i in range(62)], dtype=np.int64)
+
+
 def _quad_class(counts: np.ndarray) -> np.ndarray:
     """Slot width in 4-entry quads of rows with ``counts`` entries: 0, 1, 2, 4, 8, ..."""
     quads = (np.asarray(counts, dtype=np.int64) + 3) // 4
@@ -166,7 +174,7 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
         if use_slots:  # buckets of equal padded width (power-of-two quads)
             bucket = _quad_class(counts[perm])
         else:
-            bucket = np.ceil(np.log2(counts[perm] + 1.0)).astype(np.int64)
+            bucket = _bit_length(counts[perm])
         perm = perm[_stable_argsort(-bucket if long_first else bucket)]
     heavy_mask = counts[perm] > heavy_threshold
     perm = np.concatenate((perm[~heavy_mask], perm[heavy_mask]))
@@ -209,6 +217,107 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
                        int(heavy_threshold), row_ids, 4 if pad else 1, slot_table)
 
 
+def _finish_torch(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
+                  group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True,
+                  pad: bool = False, long_first: bool = True, slots: bool = False, device="cuda") -> LevelGather:
+    """``_finish`` with PyTorch on ``device`` (the GPU when the runtime builds its levels):
+    the same steps as the NumPy version, in integer arithmetic only, so the lists, row
+    pointers, processing order and slot tables are identical to it."""
+    import torch
+
+    dev = torch.device(device)
+    i64 = torch.int64
+    rows_t = torch.as_tensor(np.asarray(rows, dtype=np.int64)).to(dev)
+    ids_t = torch.as_tensor(np.asarray(ids, dtype=np.int64)).to(dev)
+    src_t = torch.as_tensor(np.asarray(src, dtype=np.int64)).to(dev)
+    grp_t = torch.as_tensor(np.asarray(group, dtype=np.int64)).to(dev)
+    n = int(num_rows)
+    if rows_t.numel():
+        order = torch.sort(rows_t, stable=True).indices
+        rows_t, ids_t, src_t, grp_t = rows_t[order], ids_t[order], src_t[order], grp_t[order]
+        if int(ids_t.max()) > nat.MAX_ID:
+            raise ValueError(f"level {level} names ids above {nat.MAX_ID}, beyond the B200 backend's limit")
+    counts = torch.bincount(rows_t, minlength=n) if rows_t.numel() else torch.zeros(n, dtype=i64, device=dev)
+    row_ptr = torch.zeros(n + 1, dtype=i64, device=dev)
+    row_ptr[1:] = torch.cumsum(counts, 0)
+    if int(row_ptr[-1]) > np.iinfo(np.int32).max:
+        raise ValueError(f"level {level} has {int(row_ptr[-1])} entries, above the 2^31-1 per-level limit")
+    start = torch.ones(ids_t.numel(), dtype=torch.bool, device=dev)
+    if ids_t.numel() > 1:
+        start[1:] = (rows_t[1:] != rows_t[:-1]) | (grp_t[1:] != grp_t[:-1])
+    entries = ids_t | (src_t << nat.SRC_SHIFT) | torch.where(start, nat.SEG_START, 0)
+    perm = torch.arange(n, dtype=i64, device=dev)
+    if locality and n > 1:
+        key = torch.full((n,), np.iinfo(np.int64).max, dtype=i64, device=dev)
+        state_pos = torch.nonzero(src_t == nat.SRC_STATE).flatten()
+        if state_pos.numel():
+            rs = rows_t[state_pos]
+            change = torch.ones(rs.numel(), dtype=torch.bool, device=dev)
+            change[:-1] = rs[1:] != rs[:-1]
+            last = torch.nonzero(change).flatten()
+            key[rs[last]] = ids_t[state_pos[last]]
+        perm = torch.sort(key, stable=True).indices
+    use_slots = slots and pad and balance
+    pow2 = torch.as_tensor(_POW2, device=dev)
+
+    def quad_class(c):
+        quads = (c + 3) // 4
+        width = torch.ones_like(quads)
+        while bool((width < quads).any()):
+            width = torch.where(width < quads, width * 2, width)
+        return torch.where(quads == 0, torch.zeros_like(width), width)
+
+    if balance and n > 1:
+        c = counts[perm]
+        bucket = quad_class(c) if use_slots else torch.searchsorted(pow2, c, right=True)
+        perm = perm[torch.sort(-bucket if long_first else bucket, stable=True).indices]
+    heavy_mask = counts[perm] > int(heavy_threshold)
+    perm = torch.cat((perm[~heavy_mask], perm[heavy_mask]))
+    num_heavy = int(heavy_mask.sum())
+    row_ids = None
+    if not torch.equal(perm, torch.arange(n, dtype=i64, device=dev)):
+        lengths = counts[perm]
+        new_ptr = torch.zeros(n + 1, dtype=i64, device=dev)
+        new_ptr[1:] = torch.cumsum(lengths, 0)
+        total = int(new_ptr[-1])
+        gather = torch.repeat_interleave(row_ptr[:-1][perm] - new_ptr[:-1], lengths, output_size=total) + \
+            torch.arange(total, dtype=i64, device=dev)
+        entries = entries[gather]
+        row_ptr, row_ids = new_ptr, perm
+    counts = row_ptr[1:] - row_ptr[:-1]
+    slot_table = None
+    if pad:
+        padded = (counts + 3) // 4 * 4
+        if use_slots:
+            narrow = n - num_heavy
+            width = quad_class(counts[:narrow])
+            padded = padded.clone()
+            padded[:narrow] = 4 * width
+            if narrow:
+                change = torch.ones(narrow, dtype=torch.bool, device=dev)
+                change[1:] = width[1:] != width[:-1]
+                starts = torch.nonzero(change).flatten()
+                first_entry = torch.zeros(narrow + 1, dtype=i64, device=dev)
+                first_entry[1:] = torch.cumsum(padded[:narrow], 0)
+                slot_table = torch.stack([starts, first_entry[starts], width[starts]], dim=1).cpu().numpy().astype(np.int64)
+            else:
+                slot_table = np.zeros((0, 3), dtype=np.int64)
+        new_ptr = torch.zeros(n + 1, dtype=i64, device=dev)
+        new_ptr[1:] = torch.cumsum(padded, 0)
+        out = torch.full((int(new_ptr[-1]),), nat.SRC_NULL << nat.SRC_SHIFT, dtype=i64, device=dev)
+        owner = torch.repeat_interleave(torch.arange(n, dtype=i64, device=dev), counts, output_size=entries.numel())
+        out[new_ptr[:-1][owner] + (torch.arange(entries.numel(), dtype=i64, device=dev) - row_ptr[:-1][owner])] = entries
+        entries, row_ptr = out, new_ptr
+        if int(row_ptr[-1]) > np.iinfo(np.int32).max:
+            raise ValueError(f"level {level} has {int(row_ptr[-1])} padded entries, above the 2^31-1 per-level limit")
+    if slot_table is not None and slot_table.shape[0] > nat.MAX_SLOT_BUCKETS:
+        slot_table = None
+    heavy = np.arange(n - num_heavy, n, dtype=np.int32)
+    return LevelGather(level, int(row_begin), n, row_ptr.to(torch.int32).cpu().numpy(),
+                       entries.cpu().numpy().astype(np.uint32), heavy, int(heavy_threshold),
+                       None if row_ids is None else row_ids.to(torch.int32).cpu().numpy(), 4 if pad else 1, slot_table)
+
+
 def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
     """Canonical COO of every non-empty block, keyed by (dst level, src level)."""
     out = {}
@@ -220,8 +329,11 @@ def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
 
 
 def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, locality: bool = False,
-                    balance: bool = True, pad: bool = False, long_first: bool = True, slots: bool = False) -> list[LevelGather]:
-    """Gather lists for up levels 1..h-1 (level 0 is seeded from the input)."""
+                    balance: bool = True, pad: bool = False, long_first: bool = True, slots: bool = False,
+                    device=None) -> list[LevelGather]:
+    """Gather lists for up levels 1..h-1 (level 0 is seeded from the input); built with
+    PyTorch on ``device`` when given (identical results), else with NumPy."""
+    finish = _finish if device is None else (lambda *a: _finish_torch(*a, device=device))
     off = np.asarray(level_offsets, dtype=np.int64)
     h = off.size - 1
     levels = []
@@ -237,7 +349,7 @@ def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, 
             src.append(np.full(r.size, s, dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
-        levels.append(_finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first, slots))
+        levels.append(finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first, slots))
     return levels
 
 
@@ -252,12 +364,14 @@ def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[
 
 def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int,
                       locality: bool = True, balance: bool = True, pad: bool = False,
-                      long_first: bool = True, slots: bool = False) -> list[LevelGather]:
-    """Gather lists for down levels h-1..0 in execution order.
+                      long_first: bool = True, slots: bool = False, device=None) -> list[LevelGather]:
+    """Gather lists for down levels h-1..0 in execution order (PyTorch on ``device`` when
+    given, identical results).
 
     ``sel_mut``/``sel_miss`` are (indptr, indices, num_mutations) triples; ``sel_miss`` may be
     None when no miss input is needed.
     """
+    finish = _finish if device is None else (lambda *a: _finish_torch(*a, device=device))
     off = np.asarray(level_offsets, dtype=np.int64)
     h = off.size - 1
     mut_nodes, mut_ids = _selector_by_node(sel_mut[0], sel_mut[1], sel_mut[2])
@@ -285,7 +399,7 @@ def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, h
             src.append(np.zeros(p.size, dtype=np.uint8))
             grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
-        levels.append(_finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
+        levels.append(finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
                               cat(grp, np.int16), heavy_threshold, locality, balance, pad, long_first, slots))
     return levels
 

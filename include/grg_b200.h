@@ -108,7 +108,8 @@ typedef enum grg_b200_bias {
  * 16-byte aligned offsets.  Rows are stored in *processing order* (chosen on the host for
  * cache locality); processing position p computes level-local row row_ids[p] (or p itself
  * when off_row_ids < 0).  Rows with more than heavy_threshold entries are the last num_heavy
- * positions (processed one CTA per row); narrow kernels cover the first num_rows - num_heavy:
+ * positions (split across a warp or a CTA per row, heavy_variant); narrow kernels cover the
+ * first num_rows - num_heavy:
  *   int32  row_ptr[num_rows + 1]     entry offsets of each processing position
  *   int32  heavy_rows[num_heavy]     the heavy positions (num_rows - num_heavy, ...)
  *   int32  row_ids[num_rows]         optional processing position -> level-local row
