@@ -616,10 +616,17 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
         Pack<T, V> part = zero_pack<T, V>();
         if (active) {
             if (a.list_align == 4) {
+                // this group's quads are q0, q0 + groups, ...: the next one's codes load while the
+                // current four rows are fetched, so a round waits on one memory latency
                 const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
-                for (int32_t q = (e0 >> 2) + grp; q < (e1 >> 2); q += groups) {
-                    const uint4 cq = __ldg(codes4 + q);
-                    const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
+                const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+                const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+                const int32_t q1 = e1 >> 2;
+                int32_t q = (e0 >> 2) + grp;
+                uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
+                for (; q < q1; q += groups) {
+                    const uint4 nxt = q + groups < q1 ? __ldg(codes4 + q + groups) : null4;
+                    const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
                     Pack<T, V> val[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
@@ -628,6 +635,7 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) add_into(part, val[u]);
+                    cur = nxt;
                 }
             } else {
                 constexpr int UW = 4;
