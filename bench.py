@@ -11,13 +11,21 @@ ops' shared ``io0`` buffer).  Metric: edge·RHS/s = steps · 2·E·k / device ti
   the working set (~0.8 GB of gather lists and node rows) exceeds the 126 MB L2, so no L2
   flush is needed between steps.
 * ``e2e``: the same steps through the public prepared-op API with the inputs copied from
-  pinned host memory and both outputs copied back every step.
+  pinned host memory and both outputs copied back every step; ``--e2e-inflight`` steps (2)
+  run at once, each on its own runtime and stream, so one step's copies overlap another's
+  kernels.
 * ``roofline``: the level gather kernels timed live (events around every level launch of one
-  instrumented up+down pass); algorithmic bytes per traversal as in DESIGN.md.
+  instrumented up+down pass).  Algorithmic bytes per level: 4 per gather entry and row
+  pointer, plus each destination row written once and read once later (2·k·8); plus, for
+  down, the mutation and miss input rows read once.  ``traffic`` is the DRAM traffic of the
+  level kernels per step from the committed ncu summary (medium graph, scaled by edges).
 * ``cpu_baseline``: the oracle (SciPy restatement of the reference's ReferenceRuntime) on one
-  step of the same graph, rank 0, N=1 only.
+  step of the same graph, RHS columns split over one process per host core (up to k), rank 0,
+  N=1 only.
+* ``tiers``: RHS-block batching and mixed precision against the plain FP64 drop-in on the same
+  graph and on eight generated graphs (N=1 only; ``--no-tiers`` skips it).
 * ``--impl reference``: the reference's CPU path (the oracle port; the pure-Python reference
-  cannot be installed offline) timed on the same workload.
+  cannot be installed offline) timed on the same workload, on the same host cores.
 
 Multi-GPU (``torchrun``): every rank runs its own graph (a different seed, as a genomic region
 would be), no data-path collective; ``value`` sums the ranks' work over the max of their times.

@@ -108,8 +108,8 @@ class B200Plan:
             raise ValueError(f"narrow_variant must be in [0, 9), got {self.narrow_variant}")
         if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
             raise ValueError("narrow_variants 6-8 read padded gather lists; they need pad_lists=True")
-        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2):
-            raise ValueError(f"heavy_variant must be 0, 1 or 2, got {self.heavy_variant}")
+        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3):
+            raise ValueError(f"heavy_variant must be 0, 1, 2 or 3, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:
             raise ValueError(f"narrow_split must be in [-1, 3], got {self.narrow_split}")
         if self.schedule not in ("levels", "dataflow"):

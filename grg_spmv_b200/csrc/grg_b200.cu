@@ -594,9 +594,9 @@ constexpr int kWarpRowThreads = 256;
 // by an xor-shuffle butterfly in a fixed order, so the result is deterministic (and exact for
 // integer data), and group 0 adds the init value and stores the row.  Compared with a CTA per
 // row this keeps eight heavy rows per CTA and needs no shared memory or block barriers.
-template <typename T, int V, int INIT>
+template <typename T, int V, int INIT, int WPC = kWarpRowThreads / 32>
 __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t block) {
-    const int64_t w = block * (kWarpRowThreads / 32) + (threadIdx.x >> 5);
+    const int64_t w = block * WPC + (threadIdx.x >> 5);
     if (w >= a.num_heavy) return;  // warp-uniform
     const int lane32 = threadIdx.x & 31;
     const int64_t pos = __ldg(a.heavy_rows + w);
@@ -664,10 +664,12 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
     }
 }
 
-template <typename T, int V, int INIT>
-__global__ void __launch_bounds__(kWarpRowThreads) level_warp_kernel(LevelArgs a) {
+// WPC = heavy rows (warps) per CTA: 8, or 32 for heavy_variant 3 (consecutive rows, which
+// share sources in locality order, then share an SM's L1).
+template <typename T, int V, int INIT, int WPC = kWarpRowThreads / 32>
+__global__ void __launch_bounds__(WPC * 32) level_warp_kernel(LevelArgs a) {
     pdl_trigger();
-    warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
+    warp_heavy_rows<T, V, INIT, WPC>(a, blockIdx.x);
 }
 
 // One launch for a whole level (heavy_variant 2): the first ceil(num_heavy / 8) CTAs take the
@@ -1646,7 +1648,7 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
     if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
-    if (a->heavy_variant < 0 || a->heavy_variant > 2) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 2]", a->heavy_variant);
+    if (a->heavy_variant < 0 || a->heavy_variant > 3) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 3]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
     if (a->schedule != GRG_B200_SCHEDULE_LEVELS && a->schedule != GRG_B200_SCHEDULE_DATAFLOW)
         return fail(GRG_B200_ERR_INVALID, "unknown schedule %d", a->schedule);
@@ -1701,7 +1703,9 @@ template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, bool pdl, cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     const bool padded_variant = variant >= 6 && variant <= 8;
-    if (padded_variant && heavy_variant == 2 && !exact) {
+    // fused launch, except for all-heavy levels (e.g. down level 0, where every sample row is
+    // heavy): those run the warp kernel alone at its higher occupancy (40 registers, 6 CTAs/SM)
+    if (padded_variant && heavy_variant == 2 && !exact && narrow > 0) {
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
         const int lg = la.log2g + la.log2s;
@@ -1789,7 +1793,17 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
 #undef GRG_NARROW
         GRG_LAUNCH_CHECK("level_narrow_kernel");
     }
-    if (la.num_heavy > 0 && !exact && heavy_variant >= 1) {
+    if (la.num_heavy > 0 && !exact && heavy_variant == 3) {
+        constexpr int wpc = 32;
+        const dim3 grid(static_cast<unsigned>((la.num_heavy + wpc - 1) / wpc));
+        switch (init_mode) {
+            case 0: GRG_CUDA_TRY(launch_k(pdl, s, grid, wpc * 32, level_warp_kernel<T, V, 0, wpc>, la)); break;
+            case 1: GRG_CUDA_TRY(launch_k(pdl, s, grid, wpc * 32, level_warp_kernel<T, V, 1, wpc>, la)); break;
+            case 2: GRG_CUDA_TRY(launch_k(pdl, s, grid, wpc * 32, level_warp_kernel<T, V, 2, wpc>, la)); break;
+            default: GRG_CUDA_TRY(launch_k(pdl, s, grid, wpc * 32, level_warp_kernel<T, V, 3, wpc>, la)); break;
+        }
+        GRG_LAUNCH_CHECK("level_warp_kernel(32 rows per CTA)");
+    } else if (la.num_heavy > 0 && !exact && heavy_variant >= 1) {
         constexpr int rows_per_cta = kWarpRowThreads / 32;
         const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
         switch (init_mode) {

@@ -61,7 +61,7 @@ typedef enum grg_b200_status {
     GRG_B200_OK = 0,
     GRG_B200_ERR_INVALID = 1,     /* bad argument; nothing was launched */
     GRG_B200_ERR_CUDA = 2,        /* a CUDA runtime call failed */
-    GRG_B200_ERR_UNSUPPORTED = 3  /* valid request outside this build's limits */
+    GRG_B200_ERR_UNSUPPORTED = 3  /* valid request outside the library's limits */
 } grg_b200_status;
 
 /*
@@ -206,7 +206,8 @@ typedef struct grg_b200_traverse_args {
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
                                            reduction); 2 as 1 but in the same launch as the narrow
-                                           rows (narrow_variant 6/7/8 only; otherwise as 1).  Exact
+                                           rows (narrow_variant 6/7/8 only; otherwise as 1); 3 as 1
+                                           with 32 heavy rows (1024 threads) per CTA.  Exact
                                            order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of

@@ -75,7 +75,7 @@ def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
         assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("heavy_variant", [0, 1, 2])
+@pytest.mark.parametrize("heavy_variant", [0, 1, 2, 3])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_fast_mode_heavy_rows(group, heavy_variant, golden_data):
     """Default mode with split heavy rows (one CTA or one warp per row, the warps also fused
