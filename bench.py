@@ -84,6 +84,9 @@ def parse_args():
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
     p.add_argument("--slots", action="store_true", help="pad narrow rows to their bucket width (list offset from position)")
     p.add_argument("--pdl", action="store_true", help="launch level kernels with programmatic dependent launch")
+    p.add_argument("--budget-frac", type=float, default=1.0,
+                   help="VRAM budget as a fraction of full residency; below 1 the largest levels stream from pinned memory")
+    p.add_argument("--ring", type=int, default=4, help="ring slots when levels stream")
     p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
     p.add_argument("--schedule", choices=["levels", "dataflow"], default=None,
                    help="one launch per level, or one persistent dataflow launch per traversal")
@@ -266,6 +269,12 @@ def run_b200(args) -> None:
     stream = torch.cuda.Stream(device=device)
     layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
                               device=local_rank, stream=stream, pair=pair, precision=args.precision)
+    if args.budget_frac < 1.0:  # stream part of the level lists from pinned host memory
+        full = layout.required_budget_for_full_residency
+        layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req,
+                                  vram_budget_bytes=int(full * args.budget_frac), ring_buffer_size=args.ring,
+                                  device=local_rank, stream=stream, pair=pair, precision=args.precision)
+    streamed_bytes = sum(lp.nbytes for lp in layout.level_plans() if not lp.resident)
     t0 = time.perf_counter()
     runtime = B200Runtime(layout, use_graphs=not args.no_graphs).__enter__()
     enter_s = time.perf_counter() - t0
@@ -341,12 +350,19 @@ def run_b200(args) -> None:
         torch.cuda._sleep(100_000_000)
         for name, op in (("up", up), ("down", down)):
             args_c = op._args
-            if pair.plan_down.schedule == "dataflow":  # one persistent launch per traversal: time the whole call
+            if pair.plan_down.schedule == "dataflow" or streamed_bytes:  # time whole traversals (streamed levels
+                # live in pinned host memory until the traversal copies them into its ring)
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
                 nat.check(lib, lib.grg_b200_traverse(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "traverse")
                 b.record(stream)
-                level_launches += 3 if name == "up" else 2  # sentinel fill (+ seed) + dataflow kernel + output
+                if pair.plan_down.schedule == "dataflow":
+                    level_launches += 3 if name == "up" else 2  # sentinel fill (+ seed) + dataflow kernel + output
+                else:
+                    fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
+                    lv_arr = runtime._artifacts[0].levels[op._spec.direction].array
+                    level_launches += sum(1 + (1 if lv.num_heavy > 0 and lv.num_heavy < lv.num_rows and not fused else 0)
+                                          for lv in lv_arr) + (2 if name == "up" else 1)
                 lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
                 units = [level_units(scan, name, L, True) for L in lv_order if scan.level_sizes[L] > 0]
                 all_evs.append((name, [(a, b)], [], units))
@@ -363,7 +379,8 @@ def run_b200(args) -> None:
                 b.record(stream)
                 evs.append((a, b))
                 fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
-                level_launches += 1 + (1 if levels.array[i].num_heavy > 0 and not fused else 0)
+                lv = levels.array[i]
+                level_launches += 1 + (1 if 0 < lv.num_heavy < lv.num_rows and not fused else 0)
             if name == "up":
                 nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
             else:
@@ -382,7 +399,8 @@ def run_b200(args) -> None:
                 print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
             lv_bytes += level_bytes(units, k, vb, name, M, use_miss=True)
-    launches_per_step = level_launches + (0 if pair.plan_down.schedule == "dataflow" else 3)  # + seed_up + outputs
+    whole = pair.plan_down.schedule == "dataflow" or streamed_bytes  # seed/output already counted
+    launches_per_step = level_launches + (0 if whole else 3)  # + seed_up + outputs
     level_total_ms = level_ms["up"] + level_ms["down"]
     peak, peak_kind = measured_peak_hbm()
     achieved = lv_bytes / (level_total_ms / 1e3) / 1e9
@@ -510,7 +528,7 @@ def run_b200(args) -> None:
             "dtype": "f64" if args.precision == "plain" else "f64 sums, f32+i16 node state",
             "data": "synthetic (seeded generator with the configuration's shapes; no public GRG dataset offline)",
             "config": {"workload": f"{args.workload}: S={S}, levels={scan.num_levels}, N={grg.num_nodes}, E={E}, M={M}, "
-                                   f"1% missing, fully resident, up+down per step",
+                                   f"1% missing, {'fully resident' if not streamed_bytes else 'levels partly streamed'}, up+down per step",
                        "k": k, "precision": args.precision, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
@@ -520,7 +538,9 @@ def run_b200(args) -> None:
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},
-                       "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)"},
+                       "l2": "working set > 126 MB L2 (no flush)", "parallelism": f"replicas x{world} (one graph per GPU)",
+                       "vram_budget_frac": args.budget_frac, "streamed_bytes_per_step": int(streamed_bytes),
+                       "ring_slots": layout.allocated_ring_buffer_size},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": traffic, "traffic_unit": "bytes per up+down step (level kernels)",
                          "traffic_source": traffic_src, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
