@@ -269,11 +269,18 @@ def run_b200(args) -> None:
     stream = torch.cuda.Stream(device=device)
     layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
                               device=local_rank, stream=stream, pair=pair, precision=args.precision)
-    if args.budget_frac < 1.0:  # stream part of the level lists from pinned host memory
-        full = layout.required_budget_for_full_residency
-        layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req,
-                                  vram_budget_bytes=int(full * args.budget_frac), ring_buffer_size=args.ring,
-                                  device=local_rank, stream=stream, pair=pair, precision=args.precision)
+    budget, ring = 0, 0
+    if args.budget_frac < 1.0:  # keep about this fraction of the level lists resident, stream the rest
+        level_bytes = layout.bytes_by_category["resident_sparse"]
+        budget, ring = int(layout.required_budget_for_full_residency - (1.0 - args.budget_frac) * level_bytes), args.ring
+        for _ in range(40):  # the ring slots come out of the same budget: grow it until the plan fits
+            try:
+                layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=budget,
+                                          ring_buffer_size=ring, device=local_rank, stream=stream, pair=pair,
+                                          precision=args.precision)
+                break
+            except ValueError:
+                budget = int(budget + 0.02 * level_bytes)
     streamed_bytes = sum(lp.nbytes for lp in layout.level_plans() if not lp.resident)
     t0 = time.perf_counter()
     runtime = B200Runtime(layout, use_graphs=not args.no_graphs).__enter__()
@@ -414,8 +421,8 @@ def run_b200(args) -> None:
         extra_runtimes = []
         for _ in range(max(args.e2e_inflight, 1) - 1):
             s2 = torch.cuda.Stream(device=device)
-            lay2 = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0,
-                                    ring_buffer_size=0, device=local_rank, stream=s2, pair=pair, precision=args.precision)
+            lay2 = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=budget,
+                                    ring_buffer_size=ring, device=local_rank, stream=s2, pair=pair, precision=args.precision)
             rt2 = B200Runtime(lay2, use_graphs=not args.no_graphs).__enter__()
             extra_runtimes.append(rt2)
             (g2,) = rt2.grgs
