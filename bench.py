@@ -94,6 +94,13 @@ def parse_args():
                    help="node state in FP64 (plain) or FP32 + 16-bit correction with FP64 sums (mixed)")
     p.add_argument("--row-order-up", choices=["natural", "locality"], default=None)
     p.add_argument("--row-order-down", choices=["natural", "locality"], default=None)
+    p.add_argument("--apps", action="store_true",
+                   help="time the application harnesses instead (randomized PCA on this graph; block CG on a "
+                        "streamed graph of the large configuration's shape) and print their JSON line")
+    p.add_argument("--apps-scale", type=float, default=0.1,
+                   help="size of the CG graph vs the large configuration (1M samples, 60M nodes, 600M edges, "
+                        "20M mutations); its VRAM budget scales with it (16 GB at 1.0)")
+    p.add_argument("--apps-artifact", default=None, help=".grg_spmv for the CG graph (generated there first if missing)")
     return p.parse_args()
 
 
@@ -783,10 +790,155 @@ def run_reference(args) -> None:
     print(json.dumps(line))
 
 
+def large_spec(scale: float):
+    """The streamed large configuration (1M haploid samples, 60 internal levels, 60M nodes,
+    ~600M edges, 20M mutations, 1% missing) from the same generator, every count times
+    ``scale``."""
+    from grg_spmv_b200.synth import SynthSpec
+
+    return SynthSpec(num_samples=int(1_000_000 * scale), num_levels=60, num_nodes=int(60_000_000 * scale),
+                     num_mutations=int(20_000_000 * scale), children=(2, 22), miss_fraction=0.01, seed=0)
+
+
+def run_apps(args) -> None:
+    """Application harnesses on one GPU, one JSON line.
+
+    * ``pca``: randomized PCA (``randomized_eigh``: 10 power iterations of Zᵀ(Z V) with a block
+      of 64 vectors, FP64 QR and Rayleigh-Ritz) on the bench graph, with the node state in plain
+      FP64 and in the mixed format; eigenvalue agreement between the two.
+    * ``cg``: block CG on (Z Zᵀ / M + 0.5 I) x = b, 16 right-hand sides, 50 iterations, FP64
+      dot products and residuals, on a graph of the large configuration's shape scaled by
+      ``--apps-scale``, with the mixed node state and a VRAM budget of 16 GB x scale and 4 ring
+      slots, so the largest level lists stream from pinned host memory every traversal; the same
+      solve fully resident in plain FP64 gives the reference solution and its time.
+    Each timed region is bracketed by device synchronisation (CUDA events on the runtime's
+    stream plus the host clock: CG reads its residuals on the host every iteration, as the
+    reference's solver does)."""
+    import torch
+
+    from grg_spmv_b200 import RuntimeRequirements, scan_grg_spmv
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+    from grg_spmv_b200.synth import write_synthetic_artifact
+    from grg_spmv_b200.xtx import StandardizedXTX, StandardizedXXT, conj_grad_solve, randomized_eigh
+
+    device = torch.device("cuda", 0)
+    torch.cuda.set_device(device)
+
+    def requirements(q):
+        return RuntimeRequirements(max_k_up=q, max_k_down=q, need_down_miss_input=True, need_up_miss_output=True,
+                                   need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
+
+    def timed(stream, fn):
+        torch.cuda.synchronize(device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        a.record(stream)
+        res = fn()
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        return res, a.elapsed_time(b), (time.perf_counter() - t0) * 1e3
+
+    out = {"metric": "GRG application harnesses (randomized PCA, block CG)", "n_gpus": 1, "data": "synthetic",
+           "dtype": "f64 (plain) / f64 sums with f32+i16 node state (mixed)"}
+
+    # Randomized PCA on the bench graph.
+    path, gen_s = make_artifact(args, 0)
+    scan = scan_grg_spmv(path)
+    pcs, over, power = 16, 48, 10
+    q = pcs + over
+    pca = {"graph": {"num_edges": scan.num_edges, "num_nodes": scan.num_nodes, "num_mutations": scan.num_mutations,
+                     "num_samples": scan.num_samples, "generate_s": gen_s},
+           "block": q, "pcs": pcs, "power_iters": power}
+    eig = {}
+    for precision in ("plain", "mixed"):
+        stream = torch.cuda.Stream(device=device)
+        layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=requirements(q), vram_budget_bytes=0,
+                                  ring_buffer_size=0, device=0, stream=stream, precision=precision, emit_all_nodes=False)
+        with B200Runtime(layout) as rt, torch.cuda.stream(stream):
+            (grg,) = rt.grgs
+            op = StandardizedXTX(rt, grg, q)
+            randomized_eigh(op, pcs, oversample=over, power_iters=1, seed=3)  # warm-up (graph capture, tuning)
+            (values, _), ms, wall_ms = timed(stream, lambda: randomized_eigh(op, pcs, oversample=over, power_iters=power, seed=3))
+            applies = power + 2
+            work = applies * 2.0 * grg.num_edges * q
+            eig[precision] = values.cpu().numpy()
+            pca[precision] = {"ms": ms, "wall_ms": wall_ms, "operator_applies": applies,
+                              "edge_rhs_per_s": work / (ms / 1e3), "top_eigenvalues": [float(v) for v in eig[precision][:4]]}
+        del op, rt
+        torch.cuda.empty_cache()
+    pca["max_rel_eigenvalue_diff_mixed_vs_plain"] = float(np.max(np.abs(eig["mixed"] - eig["plain"]) / np.abs(eig["plain"])))
+    out["pca"] = pca
+
+    # Block CG on the streamed large-shaped graph.
+    scale = float(args.apps_scale)
+    cg_path = Path(args.apps_artifact) if args.apps_artifact else Path(tempfile.mkdtemp(prefix="grg_apps_")) / f"large_{scale:g}.grg_spmv"
+    gen_s = 0.0
+    if not cg_path.exists():
+        t0 = time.perf_counter()
+        write_synthetic_artifact(large_spec(scale), cg_path)
+        gen_s = time.perf_counter() - t0
+    scan = scan_grg_spmv(cg_path)
+    c, iters, delta = 16, 50, 0.5
+    budget = int(16e9 * scale)
+    cg = {"graph": {"num_edges": scan.num_edges, "num_nodes": scan.num_nodes, "num_mutations": scan.num_mutations,
+                    "num_samples": scan.num_samples, "num_levels": scan.num_levels, "scale_vs_configuration": scale,
+                    "generate_s": gen_s},
+          "rhs": c, "iterations": iters, "delta": delta}
+    rng = np.random.default_rng(11)
+    b_np = rng.standard_normal((scan.num_samples, c))  # haploid: individuals = samples
+    sols = {}
+
+    def plan(precision, vram, ring, stream=0):
+        return plan_b200_layout(artifacts=[cg_path], dtype=np.float64, requirements=requirements(c), vram_budget_bytes=vram,
+                                ring_buffer_size=ring, device=0, stream=stream, precision=precision, emit_all_nodes=False)
+
+    def fixed_bytes(precision):  # everything but the level lists
+        full = plan(precision, 0, 0)
+        return full.bytes_total - full.bytes_by_category["resident_sparse"]
+
+    # The configuration's budget applies to the plain FP64 layout; the mixed layout gets the same
+    # room for level lists (its node state is smaller but it adds encoded down-input rows).
+    mixed_budget = budget + fixed_bytes("mixed") - fixed_bytes("plain")
+    variants = (("plain_f64_resident", "plain", 0, 0), ("plain_f64_streamed", "plain", budget, 4),
+                ("mixed_streamed", "mixed", mixed_budget, 4))
+    for name, precision, vram, ring in variants:
+        stream = torch.cuda.Stream(device=device)
+        layout = plan(precision, vram, ring, stream)
+        streamed = sum(lp.nbytes for lp in layout.level_plans() if not lp.resident)
+        lists = sum(lp.nbytes for lp in layout.level_plans())
+        t0 = time.perf_counter()
+        with B200Runtime(layout) as rt, torch.cuda.stream(stream):
+            enter_s = time.perf_counter() - t0
+            (grg,) = rt.grgs
+            op = StandardizedXXT(rt, grg, c)
+            M = grg.num_mutations
+            b = torch.from_numpy(b_np).to(device)
+            matvec = lambda v: op.apply(v) / M + delta * v
+            conj_grad_solve(matvec, b, rel_tol=0.0, max_iter=2)  # warm-up
+            (x, it, rels), ms, wall_ms = timed(stream, lambda: conj_grad_solve(matvec, b, rel_tol=0.0, max_iter=iters))
+            sols[name] = x.cpu().numpy()
+            work = it * 2.0 * grg.num_edges * c
+            cg[name] = {"ms": ms, "wall_ms": wall_ms, "ms_per_iteration": ms / it, "iterations": it,
+                        "edge_rhs_per_s": work / (ms / 1e3), "max_rel_residual": float(rels.max()),
+                        "vram_budget_bytes": vram, "ring_slots": layout.allocated_ring_buffer_size,
+                        "bytes_total": int(layout.bytes_total), "level_list_bytes": int(lists),
+                        "streamed_list_bytes_per_iteration": int(streamed),
+                        "streamed_gb_per_s": streamed * it / (ms / 1e3) / 1e9, "runtime_enter_s": enter_s}
+        del op, rt
+        torch.cuda.empty_cache()
+    ref = sols["plain_f64_resident"]
+    for name in ("plain_f64_streamed", "mixed_streamed"):
+        cg[name]["max_rel_diff_vs_plain_resident"] = float(np.max(np.abs(sols[name] - ref)) / np.max(np.abs(ref)))
+    out["cg"] = cg
+    print(json.dumps(out))
+
+
 def main() -> None:
     args = parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.apps:
+        run_apps(args)
     else:
         run_b200(args)
 

@@ -191,6 +191,7 @@ class B200Layout:
     pair: B200PlanPair
     dtype: np.dtype
     precision: str
+    emit_all_nodes: bool
     mix_scratch_bytes: int
     requirements: object
     device: int
@@ -372,6 +373,7 @@ def plan_b200_layout(
     stream,
     pair: B200PlanPair | None = None,
     precision: str = "plain",
+    emit_all_nodes: bool = True,
 ) -> B200Layout:
     """Plan device memory for ``artifacts`` (the counterpart of ``plan_triton_layout``,
     ``pygrgl_spmv/backends/triton/backend.py:343-371``).
@@ -380,7 +382,11 @@ def plan_b200_layout(
     must be float64: inputs and outputs stay FP64) keeps the node state in 6 bytes per value,
     an FP32 value plus a 16-bit correction (relative rounding <= 2^-39 per node, integers below
     2^39 exact), with FP64 accumulation; it needs padded lists and the default (not
-    exact-order) heavy-row mode."""
+    exact-order) heavy-row mode.
+
+    ``emit_all_nodes=False`` leaves out the all-node output buffer (``max_nodes x max_k``
+    values, as large as an FP64 node state): the runtime then refuses
+    ``prepare_matmul_cuda(..., emit_all_nodes=True)``, and the budget goes to level lists."""
     dtype = np.dtype(dtype)
     if dtype not in (np.dtype(np.float32), np.dtype(np.float64)):
         raise ValueError(f"B200 runtime supports only float32/float64, got {dtype}")
@@ -403,7 +409,8 @@ def plan_b200_layout(
     return plan_layout_from_scans(
         scans=tuple(scan_grg_spmv(p) for p in paths), paths=paths, dtype=dtype, requirements=requirements,
         requested_budget=requested_budget, requested_ring=requested_ring, allow_residency=bool(allow_residency),
-        device_id=device_id, stream_ptr=stream_ptr, stream_owner=stream_owner, pair=pair, precision=precision)
+        device_id=device_id, stream_ptr=stream_ptr, stream_owner=stream_owner, pair=pair, precision=precision,
+        emit_all_nodes=emit_all_nodes)
 
 
 PRECISIONS = ("plain", "mixed")
@@ -433,7 +440,7 @@ def _plane(nbytes: int) -> int:
 
 def plan_layout_from_scans(*, scans, paths, dtype, requirements, requested_budget: int, requested_ring: int,
                            allow_residency: bool, device_id: int, stream_ptr: int, stream_owner, pair: B200PlanPair,
-                           precision: str = "plain") -> B200Layout:
+                           precision: str = "plain", emit_all_nodes: bool = True) -> B200Layout:
     """The device-independent part of the planner (exercised by the CPU tests)."""
     _check_precision(precision, dtype, pair)
     itemsize = int(np.dtype(dtype).itemsize)
@@ -477,7 +484,7 @@ def plan_layout_from_scans(*, scans, paths, dtype, requirements, requested_budge
             mix_scratch = mixed_state_bytes(max_M, max_k) * (2 if down_miss else 1)
     io0_rows = max(max_S, max_M)
     io1_rows = side_io_rows(pair, requirements, max_num_mutations=max_M, max_num_nodes=max_N)
-    aux_rows = max_N  # all-node output
+    aux_rows = max_N if emit_all_nodes else 0  # all-node output
     dense_arena = (io0_rows + io1_rows + aux_rows) * max_k * itemsize
     scratch = 256 + mix_scratch  # device error word (+ mixed-precision encoded down inputs)
     fixed = selectors + metadata + xtx + state_bytes + dense_arena + scratch
@@ -546,6 +553,7 @@ def plan_layout_from_scans(*, scans, paths, dtype, requirements, requested_budge
         pair=pair,
         dtype=np.dtype(dtype),
         precision=precision,
+        emit_all_nodes=bool(emit_all_nodes),
         mix_scratch_bytes=int(mix_scratch),
         requirements=requirements,
         device=device_id,

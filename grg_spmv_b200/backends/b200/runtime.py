@@ -213,7 +213,8 @@ class B200Runtime:
                 io1_rows = side_io_rows(lay.pair, lay.requirements, max_num_mutations=lay.max_num_mutations,
                                         max_num_nodes=lay.max_num_nodes)
                 self._io1 = None if io1_rows == 0 else torch.zeros((io1_rows, max_k), device=self.device, dtype=tdt)
-                self._aux = torch.zeros((lay.max_num_nodes, max_k), device=self.device, dtype=tdt)
+                if lay.emit_all_nodes:
+                    self._aux = torch.zeros((lay.max_num_nodes, max_k), device=self.device, dtype=tdt)
                 self._error_word = torch.zeros(64, device=self.device, dtype=torch.int32)
                 self._df_sync = torch.zeros(4, device=self.device, dtype=torch.int32)  # dataflow task counter/flags
                 self._slots = [torch.empty(int(n), device=self.device, dtype=torch.uint8) for n in lay.slot_bytes]
@@ -415,6 +416,8 @@ class B200Runtime:
             raise ValueError("UP plan is not configured")
         if spec.direction == Direction.DOWN and self.layout.pair.plan_down is None:
             raise ValueError("DOWN plan is not configured")
+        if spec.emit_all_nodes and not self.layout.emit_all_nodes:
+            raise ValueError("emit_all_nodes needs a layout planned with emit_all_nodes=True")
         return B200PreparedMatmul(self, self._artifacts[int(grg._artifact_index)], spec)
 
     def _traverse_args(self, art: _DeviceArtifact, spec, input_view, output_view, miss_view, init_vector, init_matrix, *,

@@ -182,6 +182,33 @@ def test_streamed_levels_are_exact(synth_artifact, ring):
             np.testing.assert_array_equal(grg.matmul(x, direction), oracle.matmul(x, direction))
 
 
+def test_lean_mixed_streamed_layout(synth_artifact):
+    """A layout without the all-node buffer, mixed-precision node state and levels streamed
+    through a two-slot ring (the shape of the large streamed configuration): integer-valued
+    results stay exact, and asking for an all-node output is refused."""
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(44)
+    req = _req(k=4, need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
+    full = _layout([synth_artifact], requirements=req, precision="mixed", emit_all_nodes=False)
+    sizes = sorted((lp.nbytes for lp in full.level_plans()), reverse=True)
+    fixed = full.bytes_total - full.bytes_by_category["resident_sparse"]
+    layout = _layout([synth_artifact], requirements=req, precision="mixed", emit_all_nodes=False,
+                     vram_budget_bytes=fixed + 2 * sizes[0] + sum(sizes[1:3]), ring_buffer_size=2)
+    assert not layout.emit_all_nodes and layout.bytes_by_category["ring_slots"] > 0
+    with _runtime(layout) as runtime:
+        (grg,) = runtime.grgs
+        assert runtime._aux is None
+        with pytest.raises(ValueError, match="emit_all_nodes"):
+            grg.prepare_matmul_cuda(direction="up", k=2, emit_all_nodes=True)
+        for _ in range(2):
+            x_up = _pm1(rng, (4, grg.num_samples))
+            x_down, miss = _pm1(rng, (4, grg.num_mutations)), _pm1(rng, (4, grg.num_mutations))
+            np.testing.assert_array_equal(grg.matmul(x_up, "up"), oracle.matmul(x_up, "up"))
+            np.testing.assert_array_equal(grg.matmul(x_down, "down", miss=miss.copy()),
+                                          oracle.matmul(x_down, "down", miss=miss.copy()))
+        assert runtime.device_error() == 0
+
+
 def test_hybrid_budget_is_exact(synth_artifact):
     oracle = OracleGRG(synth_artifact)
     full = _layout([synth_artifact], requirements=_req(k=2))

@@ -20,12 +20,13 @@ def _req(k=2, **kw):
     return RuntimeRequirements(**base)
 
 
-def _plan(names=("band3",), *, budget=0, ring=0, allow=True, pair=None, req=None, dtype=np.float64, precision="plain"):
+def _plan(names=("band3",), *, budget=0, ring=0, allow=True, pair=None, req=None, dtype=np.float64, precision="plain",
+          emit_all_nodes=True):
     paths = tuple(artifact_path(n) for n in names)
     return plan_layout_from_scans(scans=tuple(scan_grg_spmv(p) for p in paths), paths=paths, dtype=dtype,
                                   requirements=req or _req(), requested_budget=budget, requested_ring=ring,
                                   allow_residency=allow, device_id=0, stream_ptr=0, stream_owner=None,
-                                  pair=pair or B200PlanPair(), precision=precision)
+                                  pair=pair or B200PlanPair(), precision=precision, emit_all_nodes=emit_all_nodes)
 
 
 def _keys(layout, resident: bool):
@@ -40,6 +41,18 @@ def test_budget_zero_means_full_residency():
     assert sum(i.nbytes for i in layout.budget_items) == layout.bytes_total
     # band3: up levels 1, 2; down levels 2, 1, 0
     assert _keys(layout, True) == [("down", 0), ("down", 1), ("down", 2), ("up", 1), ("up", 2)]
+
+
+def test_lean_layout_drops_the_all_node_buffer():
+    full = _plan(names=("synth_haploid",), req=_req(k=3))
+    lean = _plan(names=("synth_haploid",), req=_req(k=3), emit_all_nodes=False)
+    scan = scan_grg_spmv(artifact_path("synth_haploid"))
+    assert full.emit_all_nodes and not lean.emit_all_nodes
+    assert full.bytes_total - lean.bytes_total == scan.num_nodes * 3 * 8
+    assert full.bytes_by_category["dense_arena"] - lean.bytes_by_category["dense_arena"] == scan.num_nodes * 3 * 8
+    # the bytes saved go to level lists: a budget that streams levels in the full layout keeps them all resident
+    assert _keys(_plan(names=("synth_haploid",), req=_req(k=3), emit_all_nodes=False, budget=lean.bytes_total, ring=1),
+                 False) == []
 
 
 def test_ring_request_with_full_residency_warns():
