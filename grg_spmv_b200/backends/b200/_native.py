@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 10
+ABI_VERSION = 11
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -57,7 +57,7 @@ SRC_SHIFT = 29
 SRC_STATE, SRC_INPUT, SRC_MISS, SRC_NULL = 0, 1, 2, 3
 ID_MASK = 0x1FFFFFFF
 MAX_ID = 0x1FFFFFFF
-NARROW_VARIANTS = 9
+NARROW_VARIANTS = 11
 
 
 class Level(ctypes.Structure):
@@ -135,7 +135,7 @@ class TraverseArgs(ctypes.Structure):
         ("schedule", ctypes.c_int32),
         ("dataflow_sync", ctypes.c_void_p),
         ("launch_flags", ctypes.c_int32),
-        ("reserved3", ctypes.c_int32),
+        ("persist_ctas", ctypes.c_int32),
     ]
 
 

@@ -83,6 +83,8 @@ class B200Plan:
     ``schedule``: "levels" (one launch per level) or "dataflow" (one persistent launch per
     traversal, rows wait only for their own sources; default mode, resident levels, padded
     lists, plain precision; other calls fall back to "levels").
+    ``persist_ctas``: with ``narrow_variant`` 9 or 10, the CTAs of a level launch's persistent
+    narrow part (each walks row groups); 0 sizes it to what the GPU holds at once.
     """
 
     exact_order: bool = False
@@ -98,22 +100,25 @@ class B200Plan:
     pdl: bool = False
     narrow_split: int = -1
     schedule: str = "levels"
+    persist_ctas: int = 0
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
         if self.row_order not in (None, "natural", "locality"):
             raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
-        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < 9:
-            raise ValueError(f"narrow_variant must be in [0, 9), got {self.narrow_variant}")
+        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < 11:
+            raise ValueError(f"narrow_variant must be in [0, 11), got {self.narrow_variant}")
         if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
-            raise ValueError("narrow_variants 6-8 read padded gather lists; they need pad_lists=True")
+            raise ValueError("narrow_variants 6-10 read padded gather lists; they need pad_lists=True")
         if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3):
             raise ValueError(f"heavy_variant must be 0, 1, 2 or 3, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:
             raise ValueError(f"narrow_split must be in [-1, 3], got {self.narrow_split}")
         if self.schedule not in ("levels", "dataflow"):
             raise ValueError(f"schedule must be 'levels' or 'dataflow', got {self.schedule!r}")
+        if int(self.persist_ctas) < 0:
+            raise ValueError(f"persist_ctas must be >= 0, got {self.persist_ctas}")
 
     def resolve_narrow_variant(self, k: int) -> int:
         """The narrow-row kernel variant used for a call with ``k`` right-hand sides."""

@@ -348,7 +348,7 @@ class B200Runtime:
         return _DeviceLevels(array=arr, keepalive=keep)
 
     # -- autotuning ------------------------------------------------------------------------------
-    TUNE_VARIANTS = (5, 6, 7, 8, 0, 1, 4)
+    TUNE_VARIANTS = (5, 6, 7, 8, 9, 10, 0, 1, 4)
 
     def _tune_direction(self, direction: Direction) -> tuple[int, int]:
         """Fastest (narrow variant, heavy variant) for ``direction`` on the first artifact at
@@ -497,6 +497,7 @@ class B200Runtime:
             heavy = 2 if a.narrow_variant >= 6 else (1 if k <= 16 else 0)
         a.heavy_variant = int(heavy)
         a.narrow_split = int(plan.narrow_split)
+        a.persist_ctas = int(plan.persist_ctas)
         a.launch_flags = nat.LAUNCH_PDL if plan.pdl else 0
         a.schedule = nat.SCHEDULE_DATAFLOW if plan.schedule == "dataflow" else nat.SCHEDULE_LEVELS
         a.dataflow_sync = _ptr(self._df_sync if df_sync is None else df_sync)

@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <type_traits>
 
@@ -684,6 +685,96 @@ __global__ void __launch_bounds__(kNarrowThreads, MB) level_fused_kernel(LevelAr
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
     else if constexpr (SPLIT) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
     else vec_rows<T, V, INIT, Q>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+}
+
+// Narrow rows of padded lists, persistent (narrow_variant 9 and 10).  The narrow CTAs of a
+// launch are capped at what the GPU holds at once, and each warp walks row groups W warps
+// apart (W = warps of the narrow part).  While a group's source rows load, the warp already
+// holds the next group's list extent and requests its first 4 codes, so a group
+// costs only its rounds of row fetches (the row pointer -> codes chain of the next group is
+// hidden behind them) and a level has no partial last wave.  The per-row arithmetic is that
+// of vec_rows, so results are bit-identical to variants 6 and 7.
+template <typename T, int V, int INIT>
+__device__ __forceinline__ void persist_rows(const LevelArgs& a, int32_t block, int32_t nblocks) {
+    // 32-bit positions and row ids: the host picks this path only for levels under 2^30 rows,
+    // and node ids are below 2^29.
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int32_t narrow = static_cast<int32_t>(a.num_rows - a.num_heavy);  // heavy positions form the suffix
+    const int rows_log = 5 - a.log2g;  // a warp holds 32 / G consecutive positions
+    const int32_t pos_stride = (nblocks * kNarrowWarps) << rows_log;
+    int32_t pos = ((block * kNarrowWarps + warp) << rows_log) + (lane >> a.log2g);
+    if (pos >= narrow) return;  // no warp-wide operations below
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    int32_t e0, e1;
+    narrow_extent(a, pos, e0, e1);
+    uint4 first = (e0 >> 2) < (e1 >> 2) ? __ldg(codes4 + (e0 >> 2)) : null4;  // static list: before the wait
+    pdl_wait();
+    T* state = static_cast<T*>(a.state);
+    const int32_t step = V << a.log2g;
+    const int32_t k = static_cast<int32_t>(a.k);
+    for (;;) {
+        // the row id is needed only by the init value and the store, after the group's rounds
+        const int32_t row = static_cast<int32_t>(level_row(a, pos));
+        const int32_t npos = pos + pos_stride;  // this lane group's next position (< 2^31: narrow + stride)
+        const bool more = npos < narrow;
+        int32_t n0 = 0, n1 = 0;
+        if (more) narrow_extent(a, npos, n0, n1);
+        uint4 nfirst = null4;
+        bool pending = more;  // the next group's first codes are not requested yet
+        for (int32_t c = glane * V; c < k; c += step) {
+            Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+            Pack<T, V> seg = zero_pack<T, V>();
+            const int32_t q1 = e1 >> 2;
+            uint4 cur = first;
+            for (int32_t q = e0 >> 2; q < q1; ++q) {
+                const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+                const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+                Pack<T, V> val[4];
+                bool valid[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const T* src = entry_row<T>(a, code[u]);
+                    valid[u] = src != nullptr;
+                    val[u] = valid[u] ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                }
+                if (pending) {  // after this round's fetches are issued: waits only on n0
+                    nfirst = (n0 >> 2) < (n1 >> 2) ? __ldg(codes4 + (n0 >> 2)) : null4;
+                    pending = false;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    if (code[u] & GRG_B200_SEG_START) {
+                        add_into(acc, seg);
+                        seg = zero_pack<T, V>();
+                    }
+                    if (valid[u]) add_into(seg, val[u]);
+                }
+                cur = nxt;
+            }
+            add_into(acc, seg);
+            st_pack(state + static_cast<int64_t>(row) * a.ld_state + c, acc);
+        }
+        if (!more) return;
+        if (pending) nfirst = (n0 >> 2) < (n1 >> 2) ? __ldg(codes4 + (n0 >> 2)) : null4;  // empty row
+        pos = npos;
+        e0 = n0;
+        e1 = n1;
+        first = nfirst;
+    }
+}
+
+// heavy_variant 2 with narrow_variant 9 (MB = 5, 48 registers) or 10 (MB = 4, 64 registers):
+// the first heavy_blocks CTAs take the heavy rows one warp each, as in level_fused_kernel; the
+// other gridDim.x - heavy_blocks CTAs are the persistent narrow part.
+template <typename T, int V, int INIT, int MB>
+__global__ void __launch_bounds__(kNarrowThreads, MB) level_persist_kernel(LevelArgs a, int64_t heavy_blocks) {
+    pdl_trigger();
+    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
+    else persist_rows<T, V, INIT>(a, static_cast<int32_t>(blockIdx.x - heavy_blocks), static_cast<int32_t>(gridDim.x - heavy_blocks));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1650,6 +1741,7 @@ int validate_common(const grg_b200_traverse_args* a) {
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
     if (a->heavy_variant < 0 || a->heavy_variant > 3) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 3]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
+    if (a->persist_ctas < 0) return fail(GRG_B200_ERR_INVALID, "persist_ctas must be >= 0, got %d", a->persist_ctas);
     if (a->schedule != GRG_B200_SCHEDULE_LEVELS && a->schedule != GRG_B200_SCHEDULE_DATAFLOW)
         return fail(GRG_B200_ERR_INVALID, "unknown schedule %d", a->schedule);
     if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
@@ -1699,10 +1791,52 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
     return la;
 }
 
+// Streaming multiprocessors of the current device (looked up once per device).
+int device_sm_count(int* out) {
+    static std::atomic<int> cache[64];
+    int device = 0;
+    GRG_CUDA_TRY(cudaGetDevice(&device));
+    if (device < 0 || device >= 64) return fail(GRG_B200_ERR_UNSUPPORTED, "device ordinal %d above 63", device);
+    int sms = cache[device].load(std::memory_order_relaxed);
+    if (sms <= 0) {
+        GRG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+        cache[device].store(sms, std::memory_order_relaxed);
+    }
+    *out = sms > 0 ? sms : 1;
+    return GRG_B200_OK;
+}
+
+// Persistent narrow part (narrow_variant 9 / 10, no row split): heavy_blocks CTAs for heavy
+// rows, then at most what the GPU holds at once (SMs x CTAs per SM of the register budget)
+// for the narrow rows.
 template <typename T, int V>
-int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, bool pdl, cudaStream_t s) {
+int launch_persist(const LevelArgs& la, int init_mode, int variant, int64_t heavy_blocks, int64_t narrow_ctas, int persist_ctas,
+                   bool pdl, cudaStream_t s) {
+    int sms = 0;
+    const int rc = device_sm_count(&sms);
+    if (rc) return rc;
+    const int64_t cap = persist_ctas > 0 ? persist_ctas : static_cast<int64_t>(sms) * (variant == 9 ? 5 : 4);
+    const dim3 grid(static_cast<unsigned>(heavy_blocks + (narrow_ctas < cap ? narrow_ctas : cap)));
+#define GRG_PERSIST(INIT)                                                                                                   \
+    if (variant == 9) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_persist_kernel<T, V, INIT, 5>, la, heavy_blocks)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_persist_kernel<T, V, INIT, 4>, la, heavy_blocks));
+    switch (init_mode) {
+        case 0: GRG_PERSIST(0) break;
+        case 1: GRG_PERSIST(1) break;
+        case 2: GRG_PERSIST(2) break;
+        default: GRG_PERSIST(3) break;
+    }
+#undef GRG_PERSIST
+    GRG_LAUNCH_CHECK("level_persist_kernel");
+    return GRG_B200_OK;
+}
+
+template <typename T, int V>
+int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, int persist_ctas, bool pdl,
+                       cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    const bool padded_variant = variant >= 6 && variant <= 8;
+    const bool padded_variant = variant >= 6 && variant <= 10;
+    const bool persist = (variant == 9 || variant == 10) && la.log2s == 0 && la.num_rows < (int64_t{1} << 30);
     // fused launch, except for all-heavy levels (e.g. down level 0, where every sample row is
     // heavy): those run the warp kernel alone at its higher occupancy (40 registers, 6 CTAs/SM)
     if (padded_variant && heavy_variant == 2 && !exact && narrow > 0) {
@@ -1710,6 +1844,9 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
         const int lg = la.log2g + la.log2s;
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
+        if (persist)
+            return launch_persist<T, V>(la, init_mode, variant, heavy_blocks, (warps + kNarrowWarps - 1) / kNarrowWarps, persist_ctas,
+                                        pdl, s);
         const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
 #define GRG_FUSED_MB(INIT, MB)                                                                                 \
     if (la.log2s > 0) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, true, MB>, la, heavy_blocks)); \
@@ -1718,7 +1855,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     if (variant == 8) {                                                                                  \
         if (la.log2s > 0) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, true, 6>, la, heavy_blocks)); \
         else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, false, 3, 2>, la, heavy_blocks));          \
-    } else if (variant == 7) {                                                                           \
+    } else if (variant == 7 || variant == 9 || variant == 10) {                                          \
         GRG_FUSED_MB(INIT, 5)                                                                            \
     } else {                                                                                             \
         GRG_FUSED_MB(INIT, 6)                                                                            \
@@ -1745,13 +1882,17 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
             default: GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, 3, true, 6>, la, 0)); break;
         }
         GRG_LAUNCH_CHECK("level_fused_kernel(split)");
+    } else if (narrow > 0 && persist) {
+        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        const int rc = launch_persist<T, V>(la, init_mode, variant, 0, (warps + kNarrowWarps - 1) / kNarrowWarps, persist_ctas, pdl, s);
+        if (rc) return rc;
     } else if (narrow > 0 && padded_variant) {
         const int lg = la.log2g;
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
 #define GRG_VEC(INIT)                                                                      \
     if (variant == 8) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 3, 2>, la)); \
-    else if (variant == 7) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 5>, la)); \
+    else if (variant == 7 || variant == 9 || variant == 10) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 5>, la)); \
     else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 6>, la));
         switch (init_mode) {
             case 0: GRG_VEC(0) break;
@@ -1936,7 +2077,7 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, a->narrow_variant, s);
     return dispatch(a, sh, [&](auto t, auto v) {
         return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant,
-                                                                   (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0, s);
+                                                                   a->persist_ctas, (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0, s);
     });
 }
 

@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 10
+#define GRG_B200_ABI_VERSION 11
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -201,7 +201,11 @@ typedef struct grg_b200_traverse_args {
                                            while the current 4 rows load; 7: as 6 with 48
                                            registers per thread (5 CTAs per SM) instead of 40;
                                            8: as 6 with 8 codes (two 16-byte loads) and 8 row
-                                           fetches in flight per round (3 CTAs per SM). */
+                                           fetches in flight per round (3 CTAs per SM); 9: as 7,
+                                           persistent: the narrow CTAs are capped at the resident
+                                           count and each warp walks row groups, loading the next
+                                           group's row pointers and first codes while the current
+                                           rows load; 10: as 9 with 64 registers (4 CTAs per SM). */
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
@@ -220,7 +224,9 @@ typedef struct grg_b200_traverse_args {
     void* dataflow_sync;                /* GRG_B200_SCHEDULE_DATAFLOW: device int32[4], 16-byte aligned;
                                            [2] holds GRG_B200_DEVICE_WAIT_TIMEOUT after a failed wait */
     int32_t launch_flags;               /* GRG_B200_LAUNCH_* bits */
-    int32_t reserved3;
+    int32_t persist_ctas;               /* narrow_variant 9/10: CTAs of a level launch's persistent
+                                           narrow part (each loops over row groups); 0 = what the
+                                           GPU holds at once (SMs x CTAs per SM) */
 } grg_b200_traverse_args;
 
 /* Level, seed and output launches of the default kernels use programmatic dependent launch:
@@ -241,7 +247,7 @@ typedef struct grg_b200_traverse_args {
 typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
 #define GRG_B200_DEVICE_WAIT_TIMEOUT 6
 
-#define GRG_B200_NARROW_VARIANTS 9
+#define GRG_B200_NARROW_VARIANTS 11
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

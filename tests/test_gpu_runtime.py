@@ -102,7 +102,7 @@ def test_up_output_aliases_down_input():
 
 
 @pytest.mark.parametrize("k", [1, 2, 3, 5, 8, 16, 33])
-@pytest.mark.parametrize("variant", [0, 4, 5, 6, 7, 8])
+@pytest.mark.parametrize("variant", [0, 4, 5, 6, 7, 8, 9, 10])
 def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     """Integer-valued inputs are exact; real-valued inputs agree to 1e-12 (default heavy-row
     reduction) — every mode of the hot path on a 60k-node graph with random node ids.  Heavy
@@ -111,7 +111,7 @@ def test_synthetic_graph_against_oracle(synth_artifact, k, variant):
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
 
     oracle = OracleGRG(synth_artifact)
-    heavy_variant = {5: 1, 6: 2, 7: 2, 8: 2}.get(variant, 0)
+    heavy_variant = {5: 1, 6: 2, 7: 2, 8: 2, 9: 2, 10: 2}.get(variant, 0)
     pair = B200PlanPair(plan_up=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant),
                         plan_down=B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy_variant))
     rng = np.random.default_rng(100 + k)
@@ -477,7 +477,7 @@ def test_dataflow_wait_times_out_with_a_status_instead_of_hanging(synth_artifact
         assert int(runtime._df_sync[2].item()) == 0
 
 
-@pytest.mark.parametrize("variant", [6, 7, 8])
+@pytest.mark.parametrize("variant", [6, 7, 8, 9, 10])
 @pytest.mark.parametrize("exact", [False, True])
 def test_slot_layout_matches_row_pointer_layout(synth_artifact, variant, exact):
     """Narrow lists located from the slot table (no row_ptr load) give bit-identical results to
@@ -506,3 +506,39 @@ def test_slot_layout_matches_row_pointer_layout(synth_artifact, variant, exact):
         np.testing.assert_array_equal(a, b)
     np.testing.assert_allclose(results[True][0], oracle.matmul(x_up, "up", init=init), rtol=1e-12, atol=1e-9)
     np.testing.assert_allclose(results[True][1], oracle.matmul(x_dn, "down", miss=miss.copy()), rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("k", [1, 8, 33])
+@pytest.mark.parametrize("variant", [9, 10])
+def test_persistent_narrow_rows_match_variant_7(synth_artifact, variant, k):
+    """The persistent narrow part (each warp walks row groups, prefetching the next group's
+    list extent and codes) is bit-identical to variant 7, which has the same per-row arithmetic;
+    small ``persist_ctas`` force every warp through many groups, including groups whose rows are
+    partly past the end of the level, with init values, miss rows and the slot layout."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    oracle = OracleGRG(synth_artifact)
+    rng = np.random.default_rng(1000 + 10 * variant + k)
+    x_up = rng.standard_normal((k, 3000))
+    init = rng.standard_normal(k)
+    results = {}
+    cases = [(7, 0, False), (variant, 1, False), (variant, 3, False), (variant, 0, False), (variant, 2, True)]
+    for narrow_variant, ctas, slots in cases:
+        plan = B200Plan(narrow_variant=narrow_variant, heavy_threshold=24, heavy_variant=2, narrow_split=0,
+                        persist_ctas=ctas, slots=slots)
+        with _runtime(_layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=B200PlanPair(plan_up=plan, plan_down=plan))) as runtime:
+            (grg,) = runtime.grgs
+            assert grg.num_samples == x_up.shape[1]
+            if "x_dn" not in results:
+                results["x_dn"] = rng.standard_normal((k, grg.num_mutations))
+                results["miss"] = rng.standard_normal((k, grg.num_mutations))
+            x_dn, miss = results["x_dn"], results["miss"]
+            results[(narrow_variant, ctas, slots)] = (grg.matmul(x_up, "up", init=init), grg.matmul(x_up, "up", init="xtx"),
+                                                      grg.matmul(x_dn, "down", miss=miss.copy()))
+            assert runtime.device_error() == 0
+    base = results[(7, 0, False)]
+    for case in cases[1:]:
+        for got, want in zip(results[case], base):
+            np.testing.assert_array_equal(got, want, err_msg=str(case))
+    np.testing.assert_allclose(base[0], oracle.matmul(x_up, "up", init=init), rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(base[2], oracle.matmul(results["x_dn"], "down", miss=results["miss"].copy()), rtol=1e-12, atol=1e-9)
