@@ -11,7 +11,7 @@ ops' shared ``io0`` buffer).  Metric: edge·RHS/s = steps · 2·E·k / device ti
   the working set (~0.8 GB of gather lists and node rows) exceeds the 126 MB L2, so no L2
   flush is needed between steps.
 * ``e2e``: the same steps through the public prepared-op API with the inputs copied from
-  pinned host memory and both outputs copied back every step; ``--e2e-inflight`` steps (2)
+  pinned host memory and both outputs copied back every step; ``--e2e-inflight`` steps (4)
   run at once, each on its own runtime and stream, so one step's copies overlap another's
   kernels.
 * ``roofline``: the level gather kernels timed live (events around every level launch of one
@@ -64,7 +64,7 @@ def parse_args():
     p.add_argument("--exact-order", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--e2e-inflight", type=int, default=2, help="end-to-end steps in flight (one runtime and stream each)")
+    p.add_argument("--e2e-inflight", type=int, default=4, help="end-to-end steps in flight (one runtime and stream each)")
     p.add_argument("--no-tiers", action="store_true",
                    help="skip the batched / mixed-precision comparison on uneven RHS blocks (runs at N=1 only)")
     p.add_argument("--tier-blocks", default="1,3,16,64,256", help="RHS block widths of the tier comparison")
@@ -278,8 +278,8 @@ def run_b200(args) -> None:
                               device=local_rank, stream=stream, pair=pair, precision=args.precision)
     budget, ring = 0, 0
     if args.budget_frac < 1.0:  # keep about this fraction of the level lists resident, stream the rest
-        level_bytes = layout.bytes_by_category["resident_sparse"]
-        budget, ring = int(layout.required_budget_for_full_residency - (1.0 - args.budget_frac) * level_bytes), args.ring
+        list_bytes = layout.bytes_by_category["resident_sparse"]
+        budget, ring = int(layout.required_budget_for_full_residency - (1.0 - args.budget_frac) * list_bytes), args.ring
         for _ in range(40):  # the ring slots come out of the same budget: grow it until the plan fits
             try:
                 layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=budget,
@@ -287,7 +287,7 @@ def run_b200(args) -> None:
                                           precision=args.precision)
                 break
             except ValueError:
-                budget = int(budget + 0.02 * level_bytes)
+                budget = int(budget + 0.02 * list_bytes)
     streamed_bytes = sum(lp.nbytes for lp in layout.level_plans() if not lp.resident)
     t0 = time.perf_counter()
     runtime = B200Runtime(layout, use_graphs=not args.no_graphs).__enter__()
@@ -792,25 +792,24 @@ def run_reference(args) -> None:
 
 def large_spec(scale: float):
     """The streamed large configuration (1M haploid samples, 60 internal levels, 60M nodes,
-    ~600M edges, 20M mutations, 1% missing) from the same generator, every count times
-    ``scale``."""
+    ~600M edges, 20M mutations) from the same generator, every count times ``scale``."""
     from grg_spmv_b200.synth import SynthSpec
 
     return SynthSpec(num_samples=int(1_000_000 * scale), num_levels=60, num_nodes=int(60_000_000 * scale),
-                     num_mutations=int(20_000_000 * scale), children=(2, 22), miss_fraction=0.01, seed=0)
+                     num_mutations=int(20_000_000 * scale), children=(2, 22), seed=0)
 
 
 def run_apps(args) -> None:
-    """Application harnesses on one GPU, one JSON line.
+    """Application harnesses on one GPU, one JSON line, both on a graph of the large
+    configuration's shape scaled by ``--apps-scale``.
 
     * ``pca``: randomized PCA (``randomized_eigh``: 10 power iterations of Zᵀ(Z V) with a block
-      of 64 vectors, FP64 QR and Rayleigh-Ritz) on the bench graph, with the node state in plain
-      FP64 and in the mixed format; eigenvalue agreement between the two.
+      of 64 vectors, FP64 QR and Rayleigh-Ritz), with the node state in plain FP64 and in the
+      mixed format; eigenvalue agreement between the two.
     * ``cg``: block CG on (Z Zᵀ / M + 0.5 I) x = b, 16 right-hand sides, 50 iterations, FP64
-      dot products and residuals, on a graph of the large configuration's shape scaled by
-      ``--apps-scale``, with the mixed node state and a VRAM budget of 16 GB x scale and 4 ring
-      slots, so the largest level lists stream from pinned host memory every traversal; the same
-      solve fully resident in plain FP64 gives the reference solution and its time.
+      dot products and residuals: fully resident in plain FP64 (the reference solution), then
+      under a VRAM budget of 16 GB x scale with 4 ring slots, so the largest level lists stream
+      from pinned host memory every traversal, in plain FP64 and with the mixed node state.
     Each timed region is bracketed by device synchronisation (CUDA events on the runtime's
     stream plus the host clock: CG reads its residuals on the host every iteration, as the
     reference's solver does)."""
@@ -825,7 +824,8 @@ def run_apps(args) -> None:
     torch.cuda.set_device(device)
 
     def requirements(q):
-        return RuntimeRequirements(max_k_up=q, max_k_down=q, need_down_miss_input=True, need_up_miss_output=True,
+        miss = bool(scan.has_missing_data)
+        return RuntimeRequirements(max_k_up=q, max_k_down=q, need_down_miss_input=miss, need_up_miss_output=miss,
                                    need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
 
     def timed(stream, fn):
@@ -841,9 +841,19 @@ def run_apps(args) -> None:
     out = {"metric": "GRG application harnesses (randomized PCA, block CG)", "n_gpus": 1, "data": "synthetic",
            "dtype": "f64 (plain) / f64 sums with f32+i16 node state (mixed)"}
 
-    # Randomized PCA on the bench graph.
-    path, gen_s = make_artifact(args, 0)
+    # The large configuration's graph (no missingness: the configuration states none, and the
+    # generator draws each mutation's missingness node independently of its carriers, so an
+    # allele frequency over non-missing samples could exceed 1 and its 1/sqrt(p(1-p)) scale be NaN).
+    scale = float(args.apps_scale)
+    path = Path(args.apps_artifact) if args.apps_artifact else Path(tempfile.mkdtemp(prefix="grg_apps_")) / f"large_{scale:g}.grg_spmv"
+    gen_s = 0.0
+    if not path.exists():
+        t0 = time.perf_counter()
+        write_synthetic_artifact(large_spec(scale), path)
+        gen_s = time.perf_counter() - t0
     scan = scan_grg_spmv(path)
+
+    # Randomized PCA.
     pcs, over, power = 16, 48, 10
     q = pcs + over
     pca = {"graph": {"num_edges": scan.num_edges, "num_nodes": scan.num_nodes, "num_mutations": scan.num_mutations,
@@ -869,20 +879,12 @@ def run_apps(args) -> None:
     pca["max_rel_eigenvalue_diff_mixed_vs_plain"] = float(np.max(np.abs(eig["mixed"] - eig["plain"]) / np.abs(eig["plain"])))
     out["pca"] = pca
 
-    # Block CG on the streamed large-shaped graph.
-    scale = float(args.apps_scale)
-    cg_path = Path(args.apps_artifact) if args.apps_artifact else Path(tempfile.mkdtemp(prefix="grg_apps_")) / f"large_{scale:g}.grg_spmv"
-    gen_s = 0.0
-    if not cg_path.exists():
-        t0 = time.perf_counter()
-        write_synthetic_artifact(large_spec(scale), cg_path)
-        gen_s = time.perf_counter() - t0
-    scan = scan_grg_spmv(cg_path)
+    # Block CG with the largest level lists streamed.
+    cg_path = path
     c, iters, delta = 16, 50, 0.5
     budget = int(16e9 * scale)
     cg = {"graph": {"num_edges": scan.num_edges, "num_nodes": scan.num_nodes, "num_mutations": scan.num_mutations,
-                    "num_samples": scan.num_samples, "num_levels": scan.num_levels, "scale_vs_configuration": scale,
-                    "generate_s": gen_s},
+                    "num_samples": scan.num_samples, "num_levels": scan.num_levels, "scale_vs_configuration": scale},
           "rhs": c, "iterations": iters, "delta": delta}
     rng = np.random.default_rng(11)
     b_np = rng.standard_normal((scan.num_samples, c))  # haploid: individuals = samples
