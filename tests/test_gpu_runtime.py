@@ -542,3 +542,37 @@ def test_persistent_narrow_rows_match_variant_7(synth_artifact, variant, k):
             np.testing.assert_array_equal(got, want, err_msg=str(case))
     np.testing.assert_allclose(base[0], oracle.matmul(x_up, "up", init=init), rtol=1e-12, atol=1e-9)
     np.testing.assert_allclose(base[2], oracle.matmul(results["x_dn"], "down", miss=results["miss"].copy()), rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("k", [2, 8])
+def test_programmatic_dependent_launch_is_bit_identical(synth_artifact, k):
+    """Level, seed and output kernels launched with and without programmatic dependent launch
+    (on by default from k = 8) give bit-identical results, through the recorded CUDA graphs."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    rng = np.random.default_rng(1300 + k)
+    results = {}
+    x_up = x_dn = miss = None
+    for pdl in (None, True, False):
+        plan = B200Plan(heavy_threshold=24, pdl=pdl)
+        with _runtime(_layout([synth_artifact], requirements=_req(k=k), pair=B200PlanPair(plan_up=plan, plan_down=plan))) as runtime:
+            (grg,) = runtime.grgs
+            if x_up is None:
+                x_up = rng.standard_normal((k, grg.num_samples))
+                x_dn, miss = rng.standard_normal((k, grg.num_mutations)), rng.standard_normal((k, grg.num_mutations))
+            outs = []
+            for _ in range(2):
+                up = grg.prepare_matmul_cuda(direction="up", k=k)
+                down = grg.prepare_matmul_cuda(direction="down", k=k, use_miss=True)
+                up.input.copy_(torch.from_numpy(x_up))
+                up()
+                outs.append(up.output.cpu().numpy())
+                down.input.copy_(torch.from_numpy(x_dn))
+                down.miss_input.copy_(torch.from_numpy(miss))
+                down()
+                outs.append(down.output.cpu().numpy())
+            results[pdl] = outs
+            assert runtime.device_error() == 0
+    for pdl in (True, False):
+        for got, want in zip(results[pdl], results[None]):
+            np.testing.assert_array_equal(got, want)

@@ -185,3 +185,10 @@ def test_planned_bytes_bound_the_built_level_blobs(name, heavy, slots):
             np.testing.assert_array_equal(lv.row_ptr[pos], entry0 + (pos - pos0) * 4 * width)
             np.testing.assert_array_equal(lv.row_ptr[pos + 1] - lv.row_ptr[pos], 4 * width)
             assert b == 0 or width < lv.slots[b - 1, 2]  # longest bucket first
+
+
+def test_programmatic_dependent_launch_defaults_on_from_k8():
+    assert not B200Plan().resolve_pdl(1) and not B200Plan().resolve_pdl(7)
+    assert B200Plan().resolve_pdl(8) and B200Plan().resolve_pdl(64)
+    assert B200Plan(pdl=False).resolve_pdl(64) is False and B200Plan(pdl=True).resolve_pdl(1) is True
+    assert B200Plan.from_dict({}).pdl is None and B200Plan.from_dict({"pdl": True}).pdl is True
