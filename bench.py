@@ -14,8 +14,9 @@ ops' shared ``io0`` buffer).  Metric: edge·RHS/s = steps · 2·E·k / device ti
   pinned host memory and both outputs copied back every step; ``--e2e-inflight`` steps (4)
   run at once, each on its own runtime and stream, so one step's copies overlap another's
   kernels.
-* ``roofline``: the level gather kernels timed live (events around every level launch of one
-  instrumented up+down pass).  Algorithmic bytes per level: 4 per gather entry and row
+* ``roofline``: the level gather kernels timed live in one instrumented up+down pass: events
+  around each direction's level launches, issued back to back as in the recorded graph (a
+  second pass with events around every launch prints the per-level breakdown to stderr).  Algorithmic bytes per level: 4 per gather entry and row
   pointer, plus each destination row written once and read once later (2·k·8); plus, for
   down, the mutation and miss input rows read once.  ``traffic`` is the DRAM traffic of the
   level kernels per step from the committed ncu summary (medium graph, scaled by edges).
@@ -385,17 +386,19 @@ def run_b200(args) -> None:
             if name == "up":
                 nat.check(lib, lib.grg_b200_seed_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "seed_up")
             levels = runtime._artifacts[0].levels[op._spec.direction]
-            evs = []
+            # One pair of events around the direction's level launches, issued back to back as in
+            # the recorded graph (events between launches would add their own gaps and break the
+            # programmatic-dependent-launch overlap); per-level events follow in a second pass.
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
             for i in range(levels.count):
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
                 nat.check(lib, lib.grg_b200_run_level(ctypes.byref(args_c), ctypes.byref(levels.array[i]),
                                                       ctypes.c_void_p(stream.cuda_stream)), "run_level")
-                b.record(stream)
-                evs.append((a, b))
                 fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                 lv = levels.array[i]
                 level_launches += 1 + (1 if 0 < lv.num_heavy < lv.num_rows and not fused else 0)
+            b.record(stream)
+            evs = [(a, b)]
             if name == "up":
                 nat.check(lib, lib.grg_b200_output_up(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "output_up")
             else:
@@ -403,17 +406,31 @@ def run_b200(args) -> None:
             lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
             units = [level_units(scan, name, L, True) for L in lv_order if scan.level_sizes[L] > 0]
             all_evs.append((name, evs, list(levels.array), units))
+        per_level = []  # diagnostic pass: events around every level launch (values are not used)
+        for name, op in (("up", up), ("down", down)):
+            if pair.plan_down.schedule == "dataflow" or streamed_bytes:
+                break
+            levels = runtime._artifacts[0].levels[op._spec.direction]
+            for i in range(levels.count):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                nat.check(lib, lib.grg_b200_run_level(ctypes.byref(op._args), ctypes.byref(levels.array[i]),
+                                                      ctypes.c_void_p(stream.cuda_stream)), "run_level")
+                b.record(stream)
+                per_level.append((name, a, b, levels.array[i]))
         torch.cuda.synchronize(device)
         for name, evs, lvs, units in all_evs:
             level_ms[name] = sum(a.elapsed_time(b) for a, b in evs)
-            if not lvs:
-                print(f"[traversal] {name} entries={sum(u[1] for u in units)} ms={level_ms[name]:.4f}", file=sys.stderr)
-            for (a, b), lv, unit in zip(evs, lvs, units):
+            print(f"[traversal] {name} entries={sum(u[1] for u in units)} ms={level_ms[name]:.4f}", file=sys.stderr)
+            lv_bytes += level_bytes(units, k, vb, name, M, use_miss=True)
+        per_level_ms = 0.0
+        for name, _, _, units in all_evs:
+            for (_, a, b, lv), unit in zip([x for x in per_level if x[0] == name], units):
                 ms = a.elapsed_time(b)
+                per_level_ms += ms
                 nbytes = level_bytes([unit], k, vb, "up", M, False)
                 print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
-            lv_bytes += level_bytes(units, k, vb, name, M, use_miss=True)
     whole = pair.plan_down.schedule == "dataflow" or streamed_bytes  # seed/output already counted
     launches_per_step = level_launches + (0 if whole else 3)  # + seed_up + outputs
     level_total_ms = level_ms["up"] + level_ms["down"]
@@ -562,7 +579,9 @@ def run_b200(args) -> None:
                                     if pair.plan_down.schedule == "dataflow" else
                                     "level gathers (one fused narrow+heavy launch per level)"),
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
-                         "level_ms_per_step": level_total_ms, "level_bytes_per_step": lv_bytes},
+                         "level_ms_per_step": level_total_ms, "level_bytes_per_step": lv_bytes,
+                         "launches_in_level_timing": level_launches,
+                         "level_ms_per_step_with_events_around_each_launch": per_level_ms or None},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(launches_per_step * args.steps),
