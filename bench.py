@@ -83,7 +83,8 @@ def parse_args():
     p.add_argument("--heavy-variant", type=int, default=None,
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
-    p.add_argument("--slots", action="store_true", help="pad narrow rows to their bucket width (list offset from position)")
+    p.add_argument("--slots", choices=["none", "up", "down", "both"], default="none",
+                   help="directions whose narrow rows are padded to their bucket width (list offset from position)")
     p.add_argument("--pdl", choices=["auto", "on", "off"], default="auto",
                    help="programmatic dependent launch of the level kernels (auto: on for k >= 8)")
     p.add_argument("--budget-frac", type=float, default=1.0,
@@ -265,16 +266,16 @@ def run_b200(args) -> None:
         extra["heavy_variant"] = args.heavy_variant
     if args.short_first:
         extra["long_first"] = False
-    if args.slots:
-        extra["slots"] = True
     if args.pdl != "auto":
         extra["pdl"] = args.pdl == "on"
     if args.narrow_split is not None:
         extra["narrow_split"] = args.narrow_split
     if args.schedule is not None:
         extra["schedule"] = args.schedule
-    pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up, **extra),
-                        plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down, **extra))
+    pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up,
+                                         slots=args.slots in ("up", "both"), **extra),
+                        plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down,
+                                           slots=args.slots in ("down", "both"), **extra))
     stream = torch.cuda.Stream(device=device)
     layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
                               device=local_rank, stream=stream, pair=pair, precision=args.precision)
@@ -565,7 +566,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "slots": pair.plan_down.slots, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split,
+                       "long_first": pair.plan_down.long_first, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
