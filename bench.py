@@ -104,6 +104,7 @@ def parse_args():
                    help="size of the CG graph vs the large configuration (1M samples, 60M nodes, 600M edges, "
                         "20M mutations); its VRAM budget scales with it (16 GB at 1.0)")
     p.add_argument("--apps-artifact", default=None, help=".grg_spmv for the CG graph (generated there first if missing)")
+    p.add_argument("--apps-only", choices=["all", "pca", "cg"], default="all", help="which application harnesses to run")
     return p.parse_args()
 
 
@@ -837,9 +838,7 @@ def run_apps(args) -> None:
     import torch
 
     from grg_spmv_b200 import RuntimeRequirements, scan_grg_spmv
-    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
     from grg_spmv_b200.synth import write_synthetic_artifact
-    from grg_spmv_b200.xtx import StandardizedXTX, StandardizedXXT, conj_grad_solve, randomized_eigh
 
     device = torch.device("cuda", 0)
     torch.cuda.set_device(device)
@@ -874,7 +873,20 @@ def run_apps(args) -> None:
         gen_s = time.perf_counter() - t0
     scan = scan_grg_spmv(path)
 
-    # Randomized PCA.
+    if args.apps_only in ("all", "pca"):
+        out["pca"] = run_pca(args, path, scan, gen_s, requirements, timed, device)
+    if args.apps_only in ("all", "cg"):
+        out["cg"] = run_cg(args, path, scan, gen_s, scale, requirements, timed, device)
+    print(json.dumps(out))
+
+
+def run_pca(args, path, scan, gen_s, requirements, timed, device) -> dict:
+    """Randomized PCA timing (see ``run_apps``)."""
+    import torch
+
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+    from grg_spmv_b200.xtx import StandardizedXTX, randomized_eigh
+
     pcs, over, power = 16, 48, 10
     q = pcs + over
     pca = {"graph": {"num_edges": scan.num_edges, "num_nodes": scan.num_nodes, "num_mutations": scan.num_mutations,
@@ -900,10 +912,16 @@ def run_apps(args) -> None:
         del op, rt
         torch.cuda.empty_cache()
     pca["max_rel_eigenvalue_diff_mixed_vs_plain"] = float(np.max(np.abs(eig["mixed"] - eig["plain"]) / np.abs(eig["plain"])))
-    out["pca"] = pca
+    return pca
 
-    # Block CG with the largest level lists streamed.
-    cg_path = path
+
+def run_cg(args, cg_path, scan, gen_s, scale, requirements, timed, device) -> dict:
+    """Block CG with the largest level lists streamed (see ``run_apps``)."""
+    import torch
+
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+    from grg_spmv_b200.xtx import StandardizedXXT, conj_grad_solve
+
     # delta = 0.5 is LMM-like (h2 about 2/3); this graph's kinship has top eigenvalues near 8e3,
     # so that system is far from converged after 50 iterations and CG amplifies rounding
     # differences between precisions.  delta = 200 converges within the 50 iterations and is
@@ -911,7 +929,8 @@ def run_apps(args) -> None:
     c, iters, delta, delta_conv = 16, 50, 0.5, 200.0
     budget = int(16e9 * scale)
     cg = {"graph": {"num_edges": scan.num_edges, "num_nodes": scan.num_nodes, "num_mutations": scan.num_mutations,
-                    "num_samples": scan.num_samples, "num_levels": scan.num_levels, "scale_vs_configuration": scale},
+                    "num_samples": scan.num_samples, "num_levels": scan.num_levels, "scale_vs_configuration": scale,
+                    "generate_s": gen_s},
           "rhs": c, "iterations": iters, "delta": delta, "delta_converging": delta_conv}
     rng = np.random.default_rng(11)
     b_np = rng.standard_normal((scan.num_samples, c))  # haploid: individuals = samples
@@ -964,8 +983,7 @@ def run_apps(args) -> None:
         cg[name]["operator_max_rel_diff_vs_plain_resident"] = rel(applied[name], applied["plain_f64_resident"])
         cg[name]["solution_max_rel_diff_vs_plain_resident"] = rel(sols[name], sols["plain_f64_resident"])
         cg[name]["solution_max_rel_diff_vs_plain_resident_delta_converging"] = rel(conv[name], conv["plain_f64_resident"])
-    out["cg"] = cg
-    print(json.dumps(out))
+    return cg
 
 
 def main() -> None:
