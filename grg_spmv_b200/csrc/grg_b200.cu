@@ -837,8 +837,6 @@ __device__ __forceinline__ RawQuad mx_load_raw(const float* hi_row, const short*
     return RawQuad{__ldg(reinterpret_cast<const float4*>(hi_row)), __ldg(reinterpret_cast<const short4*>(lo_row))};
 }
 
-__device__ __forceinline__ RawQuad zero_raw() { return RawQuad{make_float4(0.f, 0.f, 0.f, 0.f), make_short4(0, 0, 0, 0)}; }
-
 __device__ __forceinline__ void add_raw(Quad& a, const RawQuad& r) {
     a.v[0] = a.v[0] + mx_decode(r.h.x, r.l.x);
     a.v[1] = a.v[1] + mx_decode(r.h.y, r.l.y);
