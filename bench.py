@@ -91,6 +91,8 @@ def parse_args():
                    help="VRAM budget as a fraction of full residency; below 1 the largest levels stream from pinned memory")
     p.add_argument("--ring", type=int, default=4, help="ring slots when levels stream")
     p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
+    p.add_argument("--fuse-entries", type=int, default=None,
+                   help="run stretches of levels with at most this many entries as one cooperative launch (0: off)")
     p.add_argument("--schedule", choices=["levels", "dataflow"], default=None,
                    help="one launch per level, or one persistent dataflow launch per traversal")
     p.add_argument("--precision", choices=["plain", "mixed"], default="plain",
@@ -210,6 +212,21 @@ def profiled_traffic(num_edges: int, k: int, precision: str, schedule: str):
     return int(t.group(1)) * num_edges / int(e.group(1)), f"{path.relative_to(REPO)} (medium graph, scaled by edges)"
 
 
+def traversal_level_launches(levels, fused_heavy: bool, fuse_entries: int) -> int:
+    """Kernel launches of a traversal's levels: one per level (two when heavy rows run apart),
+    with each stretch of two or more resident levels of at most ``fuse_entries`` entries as one."""
+    launches, run = 0, 0
+    for lv in levels:
+        if lv.num_rows == 0:
+            continue
+        if fuse_entries > 0 and lv.ring_slot < 0 and lv.num_entries <= fuse_entries and run < 48:
+            run += 1
+            continue
+        launches += (1 if run >= 2 else run) + 1 + (1 if 0 < lv.num_heavy < lv.num_rows and not fused_heavy else 0)
+        run = 0
+    return launches + (1 if run >= 2 else run)
+
+
 def level_units(scan, direction: str, level: int, use_miss: bool) -> tuple[int, int]:
     """(rows, gather entries) of one level from the artifact scan (real edges, no padding)."""
     from grg_spmv_b200.backends.b200.structures import down_entry_bound, up_entry_bound
@@ -271,6 +288,8 @@ def run_b200(args) -> None:
         extra["pdl"] = args.pdl == "on"
     if args.narrow_split is not None:
         extra["narrow_split"] = args.narrow_split
+    if args.fuse_entries is not None:
+        extra["fuse_entries"] = args.fuse_entries
     if args.schedule is not None:
         extra["schedule"] = args.schedule
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up,
@@ -366,10 +385,11 @@ def run_b200(args) -> None:
         # Hold the stream for ~50 ms so the host enqueues every launch and event before the
         # GPU reaches them: event deltas then time kernels, not host launch latency.
         torch.cuda._sleep(100_000_000)
+        whole_traversals = pair.plan_down.schedule == "dataflow" or streamed_bytes or pair.plan_down.fuse_entries > 0
         for name, op in (("up", up), ("down", down)):
             args_c = op._args
-            if pair.plan_down.schedule == "dataflow" or streamed_bytes:  # time whole traversals (streamed levels
-                # live in pinned host memory until the traversal copies them into its ring)
+            if whole_traversals:  # streamed levels live in pinned host memory until the traversal copies
+                # them into its ring; fused level runs are formed by the traversal
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
                 nat.check(lib, lib.grg_b200_traverse(ctypes.byref(args_c), ctypes.c_void_p(stream.cuda_stream)), "traverse")
@@ -379,8 +399,7 @@ def run_b200(args) -> None:
                 else:
                     fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                     lv_arr = runtime._artifacts[0].levels[op._spec.direction].array
-                    level_launches += sum(1 + (1 if lv.num_heavy > 0 and lv.num_heavy < lv.num_rows and not fused else 0)
-                                          for lv in lv_arr) + (2 if name == "up" else 1)
+                    level_launches += traversal_level_launches(lv_arr, fused, int(op._args.fuse_entries)) + (2 if name == "up" else 1)
                 lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
                 units = [level_units(scan, name, L, True) for L in lv_order if scan.level_sizes[L] > 0]
                 all_evs.append((name, [(a, b)], [], units))
@@ -411,7 +430,7 @@ def run_b200(args) -> None:
         per_level = []  # diagnostic pass: events around every level launch (values are not used)
         for name, op in (("up", up), ("down", down)):
             if pair.plan_down.schedule == "dataflow" or streamed_bytes:
-                break
+                break  # (fused level runs: the per-level breakdown shows the unfused launches)
             levels = runtime._artifacts[0].levels[op._spec.direction]
             for i in range(levels.count):
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -433,7 +452,7 @@ def run_b200(args) -> None:
                 nbytes = level_bytes([unit], k, vb, "up", M, False)
                 print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
-    whole = pair.plan_down.schedule == "dataflow" or streamed_bytes  # seed/output already counted
+    whole = whole_traversals  # seed/output already counted
     launches_per_step = level_launches + (0 if whole else 3)  # + seed_up + outputs
     level_total_ms = level_ms["up"] + level_ms["down"]
     peak, peak_kind = measured_peak_hbm()
@@ -567,7 +586,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split,
+                       "long_first": pair.plan_down.long_first, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",

@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 11
+ABI_VERSION = 12
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -136,6 +136,7 @@ class TraverseArgs(ctypes.Structure):
         ("dataflow_sync", ctypes.c_void_p),
         ("launch_flags", ctypes.c_int32),
         ("persist_ctas", ctypes.c_int32),
+        ("fuse_entries", ctypes.c_int64),
     ]
 
 

@@ -86,6 +86,10 @@ class B200Plan:
     lists, plain precision; other calls fall back to "levels").
     ``persist_ctas``: with ``narrow_variant`` 9 or 10, the CTAs of a level launch's persistent
     narrow part (each walks row groups); 0 sizes it to what the GPU holds at once.
+    ``fuse_entries``: > 0 runs each stretch of consecutive resident levels with at most this many
+    gather entries (default mode, plain precision, padded variants) as one cooperative launch
+    with a grid barrier between levels instead of one launch per level; results are
+    bit-identical.  0 launches every level on its own.
     """
 
     exact_order: bool = False
@@ -102,6 +106,7 @@ class B200Plan:
     narrow_split: int = -1
     schedule: str = "levels"
     persist_ctas: int = 0
+    fuse_entries: int = 0
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -120,6 +125,8 @@ class B200Plan:
             raise ValueError(f"schedule must be 'levels' or 'dataflow', got {self.schedule!r}")
         if int(self.persist_ctas) < 0:
             raise ValueError(f"persist_ctas must be >= 0, got {self.persist_ctas}")
+        if int(self.fuse_entries) < 0:
+            raise ValueError(f"fuse_entries must be >= 0, got {self.fuse_entries}")
 
     def resolve_narrow_variant(self, k: int) -> int:
         """The narrow-row kernel variant used for a call with ``k`` right-hand sides."""
@@ -143,7 +150,7 @@ class B200Plan:
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
-                   "heavy_variant", "long_first", "narrow_split", "schedule", "slots", "pdl"}
+                   "heavy_variant", "long_first", "narrow_split", "schedule", "slots", "pdl", "persist_ctas", "fuse_entries"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -154,7 +161,8 @@ class B200Plan:
                    pad_lists=bool(value.get("pad_lists", True)), heavy_variant=value.get("heavy_variant"),
                    long_first=bool(value.get("long_first", True)), narrow_split=int(value.get("narrow_split", -1)),
                    schedule=str(value.get("schedule", "levels")), slots=bool(value.get("slots", False)),
-                   pdl=None if value.get("pdl") is None else bool(value.get("pdl")))
+                   pdl=None if value.get("pdl") is None else bool(value.get("pdl")),
+                   persist_ctas=int(value.get("persist_ctas", 0)), fuse_entries=int(value.get("fuse_entries", 0)))
 
 
 @dataclass(frozen=True)

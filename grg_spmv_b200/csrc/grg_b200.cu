@@ -133,6 +133,38 @@ __device__ __forceinline__ Pack<T, V> ld_ro(const T* p) {
     return r;
 }
 
+// L2 load (rows written by other SMs during this launch must not come from a stale L1 line).
+template <typename T, int V>
+__device__ __forceinline__ Pack<T, V> ld_l2(const T* p) {
+    Pack<T, V> r;
+    if constexpr (V == 1) {
+        r.v[0] = __ldcg(p);
+    } else if constexpr (std::is_same<T, double>::value && V == 2) {
+        const double2 d = __ldcg(reinterpret_cast<const double2*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else if constexpr (std::is_same<T, float>::value && V == 2) {
+        const float2 d = __ldcg(reinterpret_cast<const float2*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+    } else {
+        const float4 d = __ldcg(reinterpret_cast<const float4*>(p));
+        r.v[0] = d.x;
+        r.v[1] = d.y;
+        r.v[2] = d.z;
+        r.v[3] = d.w;
+    }
+    return r;
+}
+
+// Source-row load of the level walkers: the read-only path, or L2 only (CG) where rows read
+// here may have been written by other SMs earlier in the same launch.
+template <typename T, int V, bool CG>
+__device__ __forceinline__ Pack<T, V> ld_src(const T* p) {
+    if constexpr (CG) return ld_l2<T, V>(p);
+    else return ld_ro<T, V>(p);
+}
+
 template <typename T, int V>
 __device__ __forceinline__ void st_pack(T* p, const Pack<T, V>& x) {
     *reinterpret_cast<Pack<T, V>*>(p) = x;
@@ -453,7 +485,7 @@ __device__ __forceinline__ void narrow_extent(const LevelArgs& a, int64_t pos, i
     }
 }
 
-template <typename T, int V, int INIT, int Q = 1>
+template <typename T, int V, int INIT, int Q = 1, bool CG = false>
 __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -499,7 +531,7 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
             for (int u = 0; u < 4 * Q; ++u) {
                 const T* src = entry_row<T>(a, code[u]);
                 valid[u] = src != nullptr;
-                val[u] = valid[u] ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                val[u] = valid[u] ? ld_src<T, V, CG>(src + c) : zero_pack<T, V>();
             }
 #pragma unroll
             for (int u = 0; u < 4 * Q; ++u) {
@@ -595,7 +627,7 @@ constexpr int kWarpRowThreads = 256;
 // by an xor-shuffle butterfly in a fixed order, so the result is deterministic (and exact for
 // integer data), and group 0 adds the init value and stores the row.  Compared with a CTA per
 // row this keeps eight heavy rows per CTA and needs no shared memory or block barriers.
-template <typename T, int V, int INIT, int WPC = kWarpRowThreads / 32>
+template <typename T, int V, int INIT, int WPC = kWarpRowThreads / 32, bool CG = false>
 __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t block) {
     const int64_t w = block * WPC + (threadIdx.x >> 5);
     if (w >= a.num_heavy) return;  // warp-uniform
@@ -632,7 +664,7 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const T* src = entry_row<T>(a, code[u]);
-                        val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                        val[u] = src ? ld_src<T, V, CG>(src + c) : zero_pack<T, V>();
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) add_into(part, val[u]);
@@ -646,7 +678,7 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
                     for (int u = 0; u < UW; ++u) {
                         const int32_t jj = j + u * groups;
                         const T* src = jj < e1 ? entry_row<T>(a, __ldg(a.entries + jj)) : nullptr;
-                        val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
+                        val[u] = src ? ld_src<T, V, CG>(src + c) : zero_pack<T, V>();
                     }
 #pragma unroll
                     for (int u = 0; u < UW; ++u) add_into(part, val[u]);
@@ -775,6 +807,75 @@ __global__ void __launch_bounds__(kNarrowThreads, MB) level_persist_kernel(Level
     pdl_trigger();
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
     else persist_rows<T, V, INIT>(a, static_cast<int32_t>(blockIdx.x - heavy_blocks), static_cast<int32_t>(gridDim.x - heavy_blocks));
+}
+
+// ---------------------------------------------------------------------------------------
+// Fused runs of small levels (traverse_args.fuse_entries > 0)
+//
+// Consecutive resident levels of at most fuse_entries entries each run as one cooperative
+// launch: every CTA walks the level's virtual CTAs (heavy-row CTAs first, then narrow-row
+// CTAs, numbered as in level_fused_kernel), then all CTAs meet at a grid barrier before the
+// next level.  Rows written earlier in the launch are read through L2 (ld.cg), so no SM can
+// use a stale L1 line.  The per-row arithmetic is that of level_fused_kernel, so results are
+// bit-identical to one launch per level.  The barrier wait is bounded: after
+// kBarrierSpinLimit polls a CTA records kErrWaitTimeout in sync[2] and raises the abort flag
+// sync[1], and every CTA leaves at its next barrier.  A cooperative launch keeps every CTA
+// resident, so a correct launch never reaches the limit.
+// ---------------------------------------------------------------------------------------
+constexpr int kRunMaxLevels = 48;
+constexpr int kBarrierSpinLimit = 1 << 22;  // polls of one barrier, each after a ~64 ns sleep
+
+struct RunArgs {
+    int32_t* sync;  // [0] barrier arrivals, [1] abort flag (both zeroed before the launch), [2] status
+    int32_t num_levels;
+    int64_t heavy_blocks[kRunMaxLevels];
+    int64_t blocks[kRunMaxLevels];  // heavy + narrow virtual CTAs of each level
+    LevelArgs lv[kRunMaxLevels];
+};
+static_assert(sizeof(RunArgs) <= 32000, "launch parameters above the 32 KB limit");
+
+// Grid barrier number `phase` (1, 2, ...): false when the run is aborted (uniform per CTA).
+__device__ __forceinline__ bool run_barrier(const RunArgs& p, int phase) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = 1;
+        __threadfence();  // this CTA's rows of the level are visible before it arrives
+        atomicAdd(p.sync, 1);
+        const int target = phase * static_cast<int>(gridDim.x);
+        volatile const int32_t* arrived = p.sync;
+        volatile const int32_t* aborted = p.sync + 1;
+        for (int spin = 0; *arrived < target; ++spin) {
+            if (*aborted) {
+                good = 0;
+                break;
+            }
+            if (spin >= kBarrierSpinLimit) {
+                atomicCAS(p.sync + 2, 0, static_cast<int32_t>(kErrWaitTimeout));
+                atomicExch(p.sync + 1, 1);
+                good = 0;
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <typename T, int V, int INIT, int MB>
+__global__ void __launch_bounds__(kNarrowThreads, MB) level_run_kernel(const __grid_constant__ RunArgs p) {
+    for (int i = 0; i < p.num_levels; ++i) {
+        const LevelArgs& a = p.lv[i];
+        const int64_t hb = p.heavy_blocks[i];
+        for (int64_t vb = blockIdx.x; vb < p.blocks[i]; vb += gridDim.x) {  // the same trip count in every thread
+            if (vb < hb) warp_heavy_rows<T, V, INIT, kWarpRowThreads / 32, true>(a, vb);
+            else vec_rows<T, V, INIT, 1, true>(a, vb - hb);
+        }
+        if (i + 1 < p.num_levels && !run_barrier(p, i + 1)) return;
+    }
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1295,30 +1396,6 @@ __device__ __forceinline__ bool any_sentinel(const Pack<T, V>& p) {
     return s;
 }
 
-// L2 load (rows written by other SMs during this launch must not come from a stale L1 line).
-template <typename T, int V>
-__device__ __forceinline__ Pack<T, V> ld_l2(const T* p) {
-    Pack<T, V> r;
-    if constexpr (V == 1) {
-        r.v[0] = __ldcg(p);
-    } else if constexpr (std::is_same<T, double>::value && V == 2) {
-        const double2 d = __ldcg(reinterpret_cast<const double2*>(p));
-        r.v[0] = d.x;
-        r.v[1] = d.y;
-    } else if constexpr (std::is_same<T, float>::value && V == 2) {
-        const float2 d = __ldcg(reinterpret_cast<const float2*>(p));
-        r.v[0] = d.x;
-        r.v[1] = d.y;
-    } else {
-        const float4 d = __ldcg(reinterpret_cast<const float4*>(p));
-        r.v[0] = d.x;
-        r.v[1] = d.y;
-        r.v[2] = d.z;
-        r.v[3] = d.w;
-    }
-    return r;
-}
-
 __device__ __forceinline__ bool df_aborted(const DfArgs& p) {
     return *reinterpret_cast<volatile const int32_t*>(p.sync + 1) != 0;
 }
@@ -1740,6 +1817,7 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->heavy_variant < 0 || a->heavy_variant > 3) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 3]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
     if (a->persist_ctas < 0) return fail(GRG_B200_ERR_INVALID, "persist_ctas must be >= 0, got %d", a->persist_ctas);
+    if (a->fuse_entries < 0) return fail(GRG_B200_ERR_INVALID, "fuse_entries must be >= 0, got %lld", (long long)a->fuse_entries);
     if (a->schedule != GRG_B200_SCHEDULE_LEVELS && a->schedule != GRG_B200_SCHEDULE_DATAFLOW)
         return fail(GRG_B200_ERR_INVALID, "unknown schedule %d", a->schedule);
     if (a->init_mode == GRG_B200_INIT_VECTOR && !a->init_vector) return fail(GRG_B200_ERR_INVALID, "init_vector is NULL");
@@ -2018,10 +2096,9 @@ int dispatch(const grg_b200_traverse_args* a, const Shape& sh, F&& f) {
     return f(float{}, std::integral_constant<int, 1>{});
 }
 
-int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level* L, const void* blob, cudaStream_t s) {
-    if (L->num_rows < 0 || L->num_heavy < 0 || L->num_entries < 0)
-        return fail(GRG_B200_ERR_INVALID, "negative level sizes");
-    if (L->num_rows == 0) return GRG_B200_OK;
+// Checked launch parameters of one non-empty level whose lists are at `blob` (run_level and
+// the fused runs share them).
+int build_level_args(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level* L, const void* blob, LevelArgs& out) {
     if (!blob) return fail(GRG_B200_ERR_INVALID, "level blob is NULL");
     if (L->row_begin < 0 || L->row_begin + L->num_rows > a->num_nodes)
         return fail(GRG_B200_ERR_INVALID, "level rows [%lld, %lld) outside the %lld nodes", (long long)L->row_begin,
@@ -2071,12 +2148,91 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
         if (sh.log2g + la.log2s > 5) la.log2s = 5 - sh.log2g;
     }
     la.heavy_threshold = L->num_heavy > 0 ? L->heavy_threshold : INT32_MAX;
+    out = la;
+    return GRG_B200_OK;
+}
+
+int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level* L, const void* blob, cudaStream_t s) {
+    if (L->num_rows < 0 || L->num_heavy < 0 || L->num_entries < 0)
+        return fail(GRG_B200_ERR_INVALID, "negative level sizes");
+    if (L->num_rows == 0) return GRG_B200_OK;
+    LevelArgs la;
+    const int rc = build_level_args(a, sh, L, blob, la);
+    if (rc) return rc;
     const bool exact = a->exact_order != 0;
     if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, a->narrow_variant, s);
     return dispatch(a, sh, [&](auto t, auto v) {
         return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant,
                                                                    a->persist_ctas, (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0, s);
     });
+}
+
+// Whether level L may join a fused run: resident, non-empty, at most fuse_entries entries,
+// and a shape the run kernel reproduces bit for bit (default mode, padded lists, heavy rows one
+// warp each, no row split).  `la` receives the level's launch parameters.
+bool run_eligible(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level& L, LevelArgs& la) {
+    if (a->fuse_entries <= 0 || a->exact_order || a->dtype == GRG_B200_MIXED || a->heavy_variant != 2) return false;
+    if (a->narrow_variant < 6 || a->narrow_variant == 8 || !a->dataflow_sync) return false;
+    if (L.ring_slot >= 0 || L.num_rows <= 0 || L.num_entries > a->fuse_entries || L.list_align != 4) return false;
+    if (L.num_heavy < 0 || L.num_heavy > L.num_rows || L.num_rows >= (int64_t{1} << 30)) return false;
+    if (build_level_args(a, sh, &L, L.blob, la) != GRG_B200_OK) return false;
+    return la.log2s == 0;
+}
+
+template <typename T, int V>
+int launch_run_typed(RunArgs& p, int init_mode, int64_t max_blocks, cudaStream_t s) {
+    int device = 0, sms = 0, per_sm = 0;
+    GRG_CUDA_TRY(cudaGetDevice(&device));
+    GRG_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    void (*kernel)(const RunArgs) = nullptr;
+    switch (init_mode) {
+        case 0: kernel = level_run_kernel<T, V, 0, 5>; break;
+        case 1: kernel = level_run_kernel<T, V, 1, 5>; break;
+        case 2: kernel = level_run_kernel<T, V, 2, 5>; break;
+        default: kernel = level_run_kernel<T, V, 3, 5>; break;
+    }
+    GRG_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kNarrowThreads, 0));
+    if (per_sm < 1) return fail(GRG_B200_ERR_UNSUPPORTED, "the fused level run kernel does not fit on an SM");
+    const int64_t resident = static_cast<int64_t>(sms) * per_sm;
+    const int64_t grid = max_blocks < resident ? max_blocks : resident;
+    // arrivals and the abort flag restart at zero; a timeout status in sync[2] stays for the host
+    GRG_CUDA_TRY(cudaMemsetAsync(p.sync, 0, 2 * sizeof(int32_t), s));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid));
+    cfg.blockDim = dim3(kNarrowThreads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;  // every CTA resident: the grid barrier can complete
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    GRG_CUDA_TRY(cudaLaunchKernelEx(&cfg, kernel, p));
+    GRG_LAUNCH_CHECK("level_run_kernel");
+    return GRG_B200_OK;
+}
+
+// Runs levels [first, first + count) (all run_eligible, launch parameters in `las`) as one
+// cooperative launch.
+int launch_run(const grg_b200_traverse_args* a, const Shape& sh, const LevelArgs* las, int count, cudaStream_t s) {
+    if (count < 1 || count > kRunMaxLevels) return fail(GRG_B200_ERR_INVALID, "fused run of %d levels", count);
+    static thread_local RunArgs p;  // about 20 KB: kept off the stack
+    std::memset(&p, 0, sizeof(p));
+    p.sync = static_cast<int32_t*>(a->dataflow_sync);
+    p.num_levels = count;
+    int64_t max_blocks = 1;
+    for (int i = 0; i < count; ++i) {
+        const LevelArgs& la = las[i];
+        const int64_t narrow = la.num_rows - la.num_heavy;
+        constexpr int rows_per_cta = kWarpRowThreads / 32;
+        const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
+        const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+        p.lv[i] = la;
+        p.heavy_blocks[i] = heavy_blocks;
+        p.blocks[i] = heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps;
+        if (p.blocks[i] > max_blocks) max_blocks = p.blocks[i];
+    }
+    return dispatch(a, sh, [&](auto t, auto v) { return launch_run_typed<decltype(t), decltype(v)::value>(p, a->init_mode, max_blocks, s); });
 }
 
 int seed_up_impl(const grg_b200_traverse_args* a, const Shape& sh, cudaStream_t s) {
@@ -2486,6 +2642,25 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
         GRG_CUDA_TRY(cudaStreamWaitEvent(a->ring->copy, a->ring->fork, 0));
     }
     for (int i = 0; i < a->num_levels; ++i) {
+        if (a->fuse_entries > 0) {  // a run of small resident levels: one cooperative launch
+            static thread_local LevelArgs run_las[kRunMaxLevels];
+            int j = i, n = 0;
+            while (j < a->num_levels && n < kRunMaxLevels) {
+                if (a->levels[j].num_rows == 0) {  // an empty level launches nothing
+                    ++j;
+                    continue;
+                }
+                if (!run_eligible(a, sh, a->levels[j], run_las[n])) break;
+                ++n;
+                ++j;
+            }
+            if (n >= 2) {
+                rc = launch_run(a, sh, run_las, n, s);
+                if (rc) return rc;
+                i = j - 1;
+                continue;
+            }
+        }
         const grg_b200_level& L = a->levels[i];
         const void* blob = L.blob;
         if (L.ring_slot >= 0 && L.num_rows > 0) {

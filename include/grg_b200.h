@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 11
+#define GRG_B200_ABI_VERSION 12
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -227,6 +227,13 @@ typedef struct grg_b200_traverse_args {
     int32_t persist_ctas;               /* narrow_variant 9/10: CTAs of a level launch's persistent
                                            narrow part (each loops over row groups); 0 = what the
                                            GPU holds at once (SMs x CTAs per SM) */
+    int64_t fuse_entries;               /* > 0 (default mode, FP64/FP32, narrow_variant 6/7/9/10,
+                                           heavy_variant 2, dataflow_sync set): runs of 2 to 48
+                                           consecutive resident levels of at most this many entries
+                                           each run as one cooperative launch with a bounded grid
+                                           barrier between levels (results bit-identical; a barrier
+                                           that gives up leaves GRG_B200_DEVICE_WAIT_TIMEOUT in
+                                           dataflow_sync[2]); 0 = one launch per level */
 } grg_b200_traverse_args;
 
 /* Level, seed and output launches of the default kernels use programmatic dependent launch:

@@ -576,3 +576,39 @@ def test_programmatic_dependent_launch_is_bit_identical(synth_artifact, k):
     for pdl in (True, False):
         for got, want in zip(results[pdl], results[None]):
             np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("k", [1, 8, 33])
+@pytest.mark.parametrize("fuse", ["small", "all-heavy"])
+def test_fused_level_runs_are_bit_identical(synth_artifact, k, fuse):
+    """Stretches of small levels run as one cooperative launch with grid barriers give the
+    same bits as one launch per level: with the default heavy threshold and the small levels
+    fused, and with heavy rows in every level (threshold 2) and every level fused."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair
+
+    rng = np.random.default_rng(1500 + k)
+    threshold, entries = (24, 20_000) if fuse == "small" else (2, 1 << 40)
+    results = {}
+    inputs = None
+    for fuse_entries in (0, entries):
+        plan = B200Plan(heavy_threshold=threshold, narrow_split=0, fuse_entries=fuse_entries)
+        with _runtime(_layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=B200PlanPair(plan_up=plan, plan_down=plan))) as runtime:
+            (grg,) = runtime.grgs
+            if inputs is None:
+                inputs = (rng.standard_normal((k, grg.num_samples)), rng.standard_normal((k, grg.num_mutations)),
+                          rng.standard_normal((k, grg.num_mutations)), rng.standard_normal(k))
+            x_up, x_dn, miss, init = inputs
+            results[fuse_entries] = [grg.matmul(x_up, "up"), grg.matmul(x_up, "up", init=init), grg.matmul(x_up, "up", init="xtx"),
+                                     grg.matmul(x_dn, "down", miss=miss.copy()), grg.matmul(x_dn, "down", init=init),
+                                     grg.matmul(_pm1(np.random.default_rng(3), (k, grg.num_individuals)), "up", by_individual=True)]
+            assert runtime.device_error() == 0
+            if fuse_entries:
+                levels = runtime._artifacts[0].levels
+                fused = [lv for d in levels for lv in levels[d].array if 0 < lv.num_entries <= fuse_entries]
+                assert len(fused) >= 4  # the runs are not empty
+    for got, want in zip(results[entries], results[0]):
+        np.testing.assert_array_equal(got, want)
+    oracle = OracleGRG(synth_artifact)
+    x_up, x_dn, miss, _ = inputs
+    np.testing.assert_allclose(results[entries][0], oracle.matmul(x_up, "up"), rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(results[entries][3], oracle.matmul(x_dn, "down", miss=miss.copy()), rtol=1e-12, atol=1e-9)
