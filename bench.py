@@ -106,7 +106,10 @@ def parse_args():
                    help="size of the CG graph vs the large configuration (1M samples, 60M nodes, 600M edges, "
                         "20M mutations); its VRAM budget scales with it (16 GB at 1.0)")
     p.add_argument("--apps-artifact", default=None, help=".grg_spmv for the CG graph (generated there first if missing)")
-    p.add_argument("--apps-only", choices=["all", "pca", "cg"], default="all", help="which application harnesses to run")
+    p.add_argument("--apps-only", choices=["all", "pca", "cg", "precision"], default="all",
+                   help="which application harnesses to run")
+    p.add_argument("--precision-artifact", default=None,
+                   help=".grg_spmv for the precision harness (diploid config-2 graph; generated there first if missing)")
     return p.parse_args()
 
 
@@ -883,6 +886,10 @@ def run_apps(args) -> None:
     # The large configuration's graph (no missingness: the configuration states none, and the
     # generator draws each mutation's missingness node independently of its carriers, so an
     # allele frequency over non-missing samples could exceed 1 and its 1/sqrt(p(1-p)) scale be NaN).
+    if args.apps_only == "precision":
+        out["precision"] = run_precision(args, timed, device)
+        print(json.dumps(out))
+        return
     scale = float(args.apps_scale)
     path = Path(args.apps_artifact) if args.apps_artifact else Path(tempfile.mkdtemp(prefix="grg_apps_")) / f"large_{scale:g}.grg_spmv"
     gen_s = 0.0
@@ -892,11 +899,90 @@ def run_apps(args) -> None:
         gen_s = time.perf_counter() - t0
     scan = scan_grg_spmv(path)
 
+    if args.apps_only == "all":
+        out["precision"] = run_precision(args, timed, device)
     if args.apps_only in ("all", "pca"):
         out["pca"] = run_pca(args, path, scan, gen_s, requirements, timed, device)
     if args.apps_only in ("all", "cg"):
         out["cg"] = run_cg(args, path, scan, gen_s, scale, requirements, timed, device)
     print(json.dumps(out))
+
+
+def run_precision(args, timed, device) -> dict:
+    """The precision configuration: the config-2 graph in its diploid variant with coalescence
+    counts, k = 32, up and down with init_xtx (the 2·coalescence-count node initialisation and
+    its endpoint bias, in FP64), N(0,1) and integer allele-count (0, 1, 2) inputs.  The node
+    state in plain FP64 and in the mixed format (FP32 + 16-bit correction, FP64 sums); device
+    time per up+down pair and the max relative error of each against the CPU oracle (FP64, the
+    reference's arithmetic) on the first 4 of the 32 columns, and of mixed against plain FP64 on
+    all 32."""
+    import torch
+
+    from grg_spmv_b200 import RuntimeRequirements
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+    from grg_spmv_b200.synth import CONFIG2, write_synthetic_artifact
+
+    path = Path(args.precision_artifact) if args.precision_artifact else Path(tempfile.mkdtemp(prefix="grg_prec_")) / "config2_diploid.grg_spmv"
+    gen_s = 0.0
+    if not path.exists():
+        t0 = time.perf_counter()
+        write_synthetic_artifact(dataclasses.replace(CONFIG2, ploidy=2, with_coalescence=True, seed=0), path)
+        gen_s = time.perf_counter() - t0
+    k, check_cols = 32, 4
+    req = RuntimeRequirements(max_k_up=k, max_k_down=k, need_down_miss_input=False, need_up_miss_output=False,
+                              need_init_vector=False, need_init_matrix=False, need_init_xtx=True)
+    rng = np.random.default_rng(21)
+    out = {"graph": {"path_kind": "config-2 generator, ploidy 2, coalescence counts", "generate_s": gen_s}, "k": k,
+           "init": "xtx", "oracle_columns": check_cols}
+    results = {}
+    for precision in ("plain", "mixed"):
+        stream = torch.cuda.Stream(device=device)
+        layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
+                                  device=0, stream=stream, precision=precision, emit_all_nodes=False)
+        with B200Runtime(layout) as rt, torch.cuda.stream(stream):
+            (grg,) = rt.grgs
+            out["graph"].update(num_edges=grg.num_edges, num_nodes=grg.num_nodes, num_mutations=grg.num_mutations,
+                                num_samples=grg.num_samples, ploidy=grg.ploidy)
+            if "inputs" not in results:
+                results["inputs"] = {
+                    "normal": (rng.standard_normal((k, grg.num_samples)), rng.standard_normal((k, grg.num_mutations))),
+                    "allele_counts": (rng.integers(0, 3, (k, grg.num_samples)).astype(np.float64),
+                                      rng.integers(0, 3, (k, grg.num_mutations)).astype(np.float64)),
+                }
+            up = grg.prepare_matmul_cuda(direction="up", k=k, init_mode="xtx")
+            down = grg.prepare_matmul_cuda(direction="down", k=k, init_mode="xtx")
+            x_up = torch.from_numpy(results["inputs"]["normal"][0]).to(device)
+            x_dn = torch.from_numpy(results["inputs"]["normal"][1]).to(device)
+
+            def pair():
+                up.input.copy_(x_up)
+                up()
+                down.input.copy_(x_dn)
+                down()
+
+            for _ in range(3):
+                pair()
+            _, ms, _ = timed(stream, lambda: [pair() for _ in range(5)])
+            out[precision] = {"ms_per_up_down": ms / 5, "edge_rhs_per_s": 2.0 * grg.num_edges * k / (ms / 5 / 1e3)}
+            for name, (xu, xd) in results["inputs"].items():
+                results[(precision, name)] = (grg.matmul(xu, "up", init="xtx"), grg.matmul(xd, "down", init="xtx"))
+        del up, down, rt
+        torch.cuda.empty_cache()
+    sys.path.insert(0, str(REPO / "oracle"))
+    from grg_oracle import OracleGRG
+
+    oracle = OracleGRG(path)
+    rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(float(np.max(np.abs(ref))), 1e-300))
+    for name, (xu, xd) in results["inputs"].items():
+        ref_up = oracle.matmul(xu[:check_cols], "up", init="xtx")
+        ref_dn = oracle.matmul(xd[:check_cols], "down", init="xtx")
+        for precision in ("plain", "mixed"):
+            got_up, got_dn = results[(precision, name)]
+            out[precision][f"max_rel_err_vs_oracle_{name}"] = max(rel(got_up[:check_cols], ref_up), rel(got_dn[:check_cols], ref_dn))
+        m_up, m_dn = results[("mixed", name)]
+        p_up, p_dn = results[("plain", name)]
+        out["mixed"][f"max_rel_err_vs_plain_f64_{name}"] = max(rel(m_up, p_up), rel(m_dn, p_dn))
+    return out
 
 
 def run_pca(args, path, scan, gen_s, requirements, timed, device) -> dict:
