@@ -192,3 +192,18 @@ def test_programmatic_dependent_launch_defaults_on_from_k8():
     assert B200Plan().resolve_pdl(8) and B200Plan().resolve_pdl(64)
     assert B200Plan(pdl=False).resolve_pdl(64) is False and B200Plan(pdl=True).resolve_pdl(1) is True
     assert B200Plan.from_dict({}).pdl is None and B200Plan.from_dict({"pdl": True}).pdl is True
+
+
+def test_kernel_shape_options_validate_and_round_trip():
+    with pytest.raises(ValueError, match="persist_ctas"):
+        B200Plan(persist_ctas=-1)
+    with pytest.raises(ValueError, match="fuse_entries"):
+        B200Plan(fuse_entries=-5)
+    with pytest.raises(ValueError, match="narrow_variant"):
+        B200Plan(narrow_variant=11)
+    with pytest.raises(ValueError, match="padded"):
+        B200Plan(narrow_variant=9, pad_lists=False)
+    plan = B200Plan.from_dict({"narrow_variant": 10, "persist_ctas": 3, "fuse_entries": 600_000, "pdl": False})
+    assert (plan.narrow_variant, plan.persist_ctas, plan.fuse_entries, plan.pdl) == (10, 3, 600_000, False)
+    with pytest.raises(ValueError, match="unknown B200Plan field"):
+        B200Plan.from_dict({"fuse": 1})
