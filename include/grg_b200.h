@@ -210,18 +210,18 @@ typedef struct grg_b200_traverse_args {
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
                                            reduction); 2 as 1 but in the same launch as the narrow
-                                           rows (narrow_variant 6/7/8 only; otherwise as 1); 3 as 1
+                                           rows (narrow_variant 6 to 10 only; otherwise as 1); 3 as 1
                                            with 32 heavy rows (1024 threads) per CTA.  Exact
                                            order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of
                                            num_mutations rows and ld_state columns */
     int64_t mix_scratch_bytes;
-    int32_t narrow_split;               /* narrow_variant 6/7/8, default mode, FP64/FP32: split each narrow
+    int32_t narrow_split;               /* narrow_variant 6 to 10, default mode, FP64/FP32: split each narrow
                                            row over 2^narrow_split lane groups (0..3), or -1 to choose
                                            per level (long rows in levels too small to fill the GPU) */
     int32_t schedule;                   /* grg_b200_schedule */
-    void* dataflow_sync;                /* GRG_B200_SCHEDULE_DATAFLOW: device int32[4], 16-byte aligned;
+    void* dataflow_sync;                /* GRG_B200_SCHEDULE_DATAFLOW and fused level runs: device int32[4], 16-byte aligned;
                                            [2] holds GRG_B200_DEVICE_WAIT_TIMEOUT after a failed wait */
     int32_t launch_flags;               /* GRG_B200_LAUNCH_* bits */
     int32_t persist_ctas;               /* narrow_variant 9/10: CTAs of a level launch's persistent
