@@ -2704,21 +2704,44 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_static_mutex;
 void* g_static_ptr[kMaxDevices] = {};
+void* g_static_ctx[kMaxDevices] = {};  // the driver context each cached address belongs to
 
-// Device address of g_static_state on the current device; looked up once per device (the
-// host symbol g_static_state is only a stand-in and must never reach a kernel).
+// The calling thread's current driver context (nullptr if none, or if the query is not
+// available).  A module's device symbols have one address per context, so a cached address
+// of g_static_state is valid only while the context it was taken in is current: after
+// cudaDeviceReset, or when a host drives the device from a context it created itself, the
+// context differs and the address is looked up again.
+void* current_context() {
+    using GetCurrentFn = int (*)(void**);
+    static const GetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<GetCurrentFn>(p);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
+// Device address of g_static_state on the current device, looked up once per device and
+// context (the host symbol g_static_state is only a stand-in and must never reach a kernel).
 int static_state_address(void** out) {
     int device = 0;
     GRG_CUDA_TRY(cudaGetDevice(&device));
     if (device < 0 || device >= kMaxDevices) return fail(GRG_B200_ERR_UNSUPPORTED, "device ordinal %d above %d", device, kMaxDevices);
+    void* ctx = current_context();  // nullptr before the runtime has made a context current
     std::lock_guard<std::mutex> lock(g_static_mutex);
-    if (!g_static_ptr[device]) {
+    if (!g_static_ptr[device] || !ctx || g_static_ctx[device] != ctx) {
         void* ptr = nullptr;
-        const cudaError_t err = cudaGetSymbolAddress(&ptr, g_static_state);
+        const cudaError_t err = cudaGetSymbolAddress(&ptr, g_static_state);  // makes the context current
         if (err != cudaSuccess || !ptr)
             return fail(GRG_B200_ERR_CUDA, "cudaGetSymbolAddress(g_static_state) on device %d failed: %s", device,
                         cudaGetErrorString(err));
         g_static_ptr[device] = ptr;
+        g_static_ctx[device] = current_context();
     }
     *out = g_static_ptr[device];
     return GRG_B200_OK;

@@ -301,7 +301,9 @@ int grg_b200_traverse(const grg_b200_traverse_args* args, void* stream);
  *     level must be resident (ring_slot < 0); otherwise GRG_B200_ERR_UNSUPPORTED.
  *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress,
  *     once per device, with that device current); make that first call before any stream
- *     capture that will contain the entry point.
+ *     capture that will contain the entry point.  The address is kept per device and driver
+ *     context: after cudaDeviceReset, or from a context the caller created itself, the next
+ *     call looks it up again (that call, too, belongs outside a capture).
  *   - All calls share the one array: calls whose work overlaps on the GPU (different streams,
  *     no ordering between them) race on it.  Calls ordered on one stream are safe; every
  *     traversal writes each node row before reading it, so nothing needs clearing. */

@@ -268,7 +268,9 @@ def _run_reference(paths):
 
 
 def main(argv) -> None:
-    reference_root = Path(argv[1] if len(argv) > 1 else "/root/reference")
+    if len(argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <path to the reference checkout>")
+    reference_root = Path(argv[1])
     _setup(reference_root)
     paths = _write_artifacts(HERE)
     store, index = _run_reference(paths)

@@ -3,10 +3,12 @@
 ``grg_b200_traverse_static`` exists for callers that cannot allocate device memory (C/FFI
 hosts without a device allocator, plugins inside another framework's memory manager, code
 that must not allocate during stream capture): it keeps the traversal's node state in a fixed
-array inside the library instead of a caller buffer.  It must give the same results as
-``grg_b200_traverse`` on the same inputs, call after call (the array is reused and keeps the
-previous call's contents), and must refuse graphs whose node state does not fit.
-This file is collected last so that a failure here does not stop the rest of the suite.
+array inside the library instead of a caller buffer.  It runs the same kernels as
+``grg_b200_traverse``, so it must give the same bits on the same inputs, call after call (the
+array is reused and keeps the previous call's contents), and must refuse what it cannot serve
+(a node state larger than the array, the mixed dtype, streamed levels) before launching
+anything.  This file is collected last so that a failure here does not stop the rest of the
+suite.
 """
 
 from __future__ import annotations
@@ -30,7 +32,8 @@ def small_artifact(tmp_path_factory):
     return path
 
 
-def test_static_state_entry_point_matches_traverse(small_artifact):
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_static_state_entry_point_matches_traverse(small_artifact, dtype):
     from grg_spmv_b200 import RuntimeRequirements
     from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
     from grg_spmv_b200.backends.b200 import _native as nat
@@ -38,19 +41,19 @@ def test_static_state_entry_point_matches_traverse(small_artifact):
     k = 4
     req = RuntimeRequirements(max_k_up=k, max_k_down=k, need_down_miss_input=True, need_up_miss_output=False,
                               need_init_vector=False, need_init_matrix=False, need_init_xtx=False)
-    layout = plan_b200_layout(artifacts=[small_artifact], dtype=np.float64, requirements=req, vram_budget_bytes=0,
+    layout = plan_b200_layout(artifacts=[small_artifact], dtype=dtype, requirements=req, vram_budget_bytes=0,
                               ring_buffer_size=0, device=0, stream=0)
     lib = nat.load_library()
     rng = np.random.default_rng(17)
-    with B200Runtime(layout, use_graphs=False) as runtime:
+    with B200Runtime(layout, use_graphs=False, check_bounds=True) as runtime:
         (grg,) = runtime.grgs
         stream = ctypes.c_void_p(runtime.stream_ptr)
         for direction in ("up", "down"):
             op = grg.prepare_matmul_cuda(direction=direction, k=k, use_miss=direction == "down")
             cols = grg.num_samples if direction == "up" else grg.num_mutations
-            x = torch.from_numpy(rng.standard_normal((k, cols))).to("cuda:0")
+            x = torch.from_numpy(rng.standard_normal((k, cols)).astype(dtype)).to("cuda:0")
             if direction == "down":
-                op.miss_input.copy_(torch.from_numpy(rng.standard_normal((k, grg.num_mutations))).to("cuda:0"))
+                op.miss_input.copy_(torch.from_numpy(rng.standard_normal((k, grg.num_mutations)).astype(dtype)).to("cuda:0"))
             # input and output share one buffer, so the input is restored before every call
             op.input.copy_(x)
             nat.check(lib, lib.grg_b200_traverse(ctypes.byref(op._args), stream), "grg_b200_traverse")
@@ -60,10 +63,27 @@ def test_static_state_entry_point_matches_traverse(small_artifact):
                 op.input.copy_(x)
                 nat.check(lib, lib.grg_b200_traverse_static(ctypes.byref(op._args), stream), "grg_b200_traverse_static")
                 torch.cuda.synchronize()
-                np.testing.assert_allclose(op.output.cpu().numpy(), expected, rtol=1e-12, atol=1e-12)
+                # the same kernels on the same inputs: the same bits
+                np.testing.assert_array_equal(op.output.cpu().numpy(), expected)
+                assert runtime.device_error() == 0, "device bounds check failed"
 
-        # A node state larger than the fixed array is refused before anything is launched.
+        # Refusals, all before anything is launched:
+        # a node state larger than the fixed array,
         big = nat.TraverseArgs.from_buffer_copy(op._args)
-        big.k = (16 << 20) // (8 * grg.num_nodes) + 1
+        big.k = (16 << 20) // (np.dtype(dtype).itemsize * grg.num_nodes) + 1
         assert lib.grg_b200_traverse_static(ctypes.byref(big), stream) == nat.ERR_UNSUPPORTED
         assert "holds at most" in nat.last_error(lib)
+        # the mixed node state,
+        mixed = nat.TraverseArgs.from_buffer_copy(op._args)
+        mixed.dtype = nat.MIXED
+        assert lib.grg_b200_traverse_static(ctypes.byref(mixed), stream) == nat.ERR_UNSUPPORTED
+        assert "FP64 and FP32" in nat.last_error(lib)
+        # and a level streamed through the ring.
+        streamed = nat.TraverseArgs.from_buffer_copy(op._args)
+        levels = (nat.Level * streamed.num_levels)(*[streamed.levels[i] for i in range(streamed.num_levels)])
+        levels[0].ring_slot = 0
+        streamed.levels = ctypes.cast(levels, ctypes.POINTER(nat.Level))
+        assert lib.grg_b200_traverse_static(ctypes.byref(streamed), stream) == nat.ERR_UNSUPPORTED
+        assert "resident" in nat.last_error(lib)
+        torch.cuda.synchronize()
+        assert runtime.device_error() == 0
