@@ -65,13 +65,14 @@ def parse_args():
     p.add_argument("--exact-order", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-k1", action="store_true", help="skip the second measurement of the same step at k = 1")
     p.add_argument("--e2e-inflight", type=int, default=4, help="end-to-end steps in flight (one runtime and stream each)")
     p.add_argument("--no-tiers", action="store_true",
                    help="skip the batched / mixed-precision comparison on uneven RHS blocks (runs at N=1 only)")
     p.add_argument("--tier-blocks", default="1,3,16,64,256", help="RHS block widths of the tier comparison")
     p.add_argument("--tier-steps", type=int, default=3)
     p.add_argument("--tier-grgs", type=int, default=8, help="graphs of the multi-graph tier (0: skip it)")
-    p.add_argument("--tier-scale", type=float, default=0.5, help="size of the multi-graph tier's graphs vs 5M-40M edges")
+    p.add_argument("--tier-scale", type=float, default=1.0, help="size of the multi-graph tier's graphs vs 5M-40M edges")
     p.add_argument("--tier-artifacts", default=None, help="directory for (reused) multi-graph tier artifacts")
     p.add_argument("--no-clocks", action="store_true", help="skip clock sampling and its untimed busy loops")
     p.add_argument("--artifact", default=None, help=".grg_spmv to use (generated there first if missing)")
@@ -186,6 +187,27 @@ class ClockSampler:
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(rows[0][2]) if rows else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def host_info(workers: int) -> dict:
+    """What every CPU number is recorded with: the host's logical CPUs and physical cores, its
+    CPU model, and the processes x threads the measurement actually used."""
+    try:
+        import psutil
+
+        physical = psutil.cpu_count(logical=False)
+    except ImportError:  # pragma: no cover - psutil is in the image
+        physical = None
+    model = None
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.lower().startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return {"host_logical_cpus": os.cpu_count(), "host_physical_cores": physical, "cpu_model": model,
+            "processes": int(workers), "threads_per_process": 1}
 
 
 def measured_peak_hbm() -> tuple[float, str]:
@@ -376,6 +398,39 @@ def run_b200(args) -> None:
         max_ms, total_work = float(mx[0]), float(t[1])
     value = total_work / (max_ms / 1e3)
 
+    # The same step at k = 1 (the configuration's other RHS width) on the same runtime.
+    k1 = None
+    if k != 1 and not args.no_k1:
+        with torch.cuda.device(device), torch.cuda.stream(stream):
+            up1 = grg.prepare_matmul_cuda(direction="up", k=1)
+            down1 = grg.prepare_matmul_cuda(direction="down", k=1, use_miss=True)
+            assert up1.output.data_ptr() == down1.input.data_ptr()
+            x1 = x_up[:1].clone()
+            down1.miss_input.copy_(torch.from_numpy(miss_np[:1]).to(device))
+
+            def step1():
+                up1.input.copy_(x1)
+                up1()
+                down1()
+
+            for _ in range(max(args.warmup, 0)):
+                step1()
+            synced_barrier()
+            a1, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a1.record(stream)
+            for _ in range(args.steps):
+                step1()
+            b1.record(stream)
+            synced_barrier()
+            ms1 = a1.elapsed_time(b1)
+        if world > 1:
+            t = torch.tensor([ms1], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms1 = float(t[0])
+        k1 = {"value": args.steps * 2.0 * E * world / (ms1 / 1e3), "unit": UNIT, "ms_per_step": ms1 / args.steps, "k": 1,
+              "launch": "same runtime, prepared ops at k = 1, CUDA-graph replay"}
+        del up1, down1
+
     # Live per-kernel timing of the level gathers (one instrumented up+down pass).
     vb = 8 if args.precision == "plain" else 6  # bytes per stored node value
     lib = runtime._lib
@@ -526,6 +581,7 @@ def run_b200(args) -> None:
     # CPU baseline (oracle) and a parity spot check of the same step, rank 0 at N=1.
     cpu = None
     max_rel = None
+    integer_check = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         workers = min(k, os.cpu_count() or 1)
         pool = ParallelOracle(path, workers)
@@ -538,7 +594,8 @@ def run_b200(args) -> None:
             pool.close()
         cpu = {"value": 2.0 * E * k / cpu_s, "unit": UNIT, "cores": workers, "kind": "port",
                "sample": f"1 up+down step (k={k}) of the same graph; SciPy ReferenceRuntime restatement, "
-                         f"{workers} processes x 1 thread (RHS columns split)", "seconds": cpu_s}
+                         f"{workers} processes x 1 thread (RHS columns split, at most one process per column)",
+               "seconds": cpu_s, **host_info(workers)}
         with torch.cuda.device(device), torch.cuda.stream(stream):
             up.input.copy_(x_up)
             up()
@@ -547,6 +604,27 @@ def run_b200(args) -> None:
             got_down = down.output.cpu().numpy()
         rel = lambda got, ref: float(np.max(np.abs(got - ref)) / max(np.max(np.abs(ref)), 1e-300))
         max_rel = max(rel(got_up, ref_up), rel(got_down, ref_down))
+        # Integer-valued inputs at full size: +-1 samples up, then down from the up output
+        # (allele-count-like sums) with 0/1/2 miss rows; exact in FP64, so the error must be 0.
+        xi = rng.choice(np.asarray([-1.0, 1.0]), size=(k, S))
+        mi = rng.integers(0, 3, size=(k, M)).astype(np.float64)
+        pool = ParallelOracle(path, workers)
+        try:
+            ref_up_i, ref_down_i = pool.step(xi, mi)
+        finally:
+            pool.close()
+        with torch.cuda.device(device), torch.cuda.stream(stream):
+            up.input.copy_(torch.from_numpy(xi).to(device))
+            down.miss_input.copy_(torch.from_numpy(mi).to(device))
+            up()
+            got_up_i = up.output.cpu().numpy()
+            down()
+            got_down_i = down.output.cpu().numpy()
+            down.miss_input.copy_(torch.from_numpy(miss_np).to(device))
+        integer_check = {"inputs": "up: +-1 samples; down: the up output with 0/1/2 miss rows", "k": k,
+                         "max_abs_err_vs_oracle": float(max(np.max(np.abs(got_up_i - ref_up_i)),
+                                                            np.max(np.abs(got_down_i - ref_down_i)))),
+                         "max_abs_value": float(max(np.max(np.abs(ref_up_i)), np.max(np.abs(ref_down_i))))}
 
     tuned = {d.value: [v, runtime._heavy_variant.get(d)] for d, v in runtime._variant.items()}
     heavy_used = {"up": int(up._args.heavy_variant), "down": int(down._args.heavy_variant)}
@@ -611,6 +689,8 @@ def run_b200(args) -> None:
             "gpu_launches": int(launches_per_step * args.steps),
             "clocks": clocks.summary(),
             "max_rel_err_vs_oracle": max_rel,
+            "integer_inputs_vs_oracle": integer_check,
+            "k1": k1,
             "tiers": tiers,
             "setup_s": {"generate": gen_s, "runtime_enter": enter_s},
         }
@@ -640,12 +720,23 @@ def make_multi_artifacts(args) -> list[Path]:
 
     root = Path(args.tier_artifacts) if args.tier_artifacts else Path(tempfile.mkdtemp(prefix="grg_tiers_"))
     root.mkdir(parents=True, exist_ok=True)
-    paths = []
+    jobs, paths = [], []
     for i, spec in enumerate(multi_grg_specs(args.tier_grgs, args.tier_scale)):
         path = root / f"multi_{args.tier_scale:g}_{i}.grg_spmv"
         if not path.exists():
-            write_synthetic_artifact(spec, path)
+            jobs.append((spec, str(path)))
         paths.append(path)
+    # The graphs are independent: a few spawned processes generate them (about 3 GB of host
+    # memory each at 40M edges).
+    workers = min(len(jobs), 4, max(1, (os.cpu_count() or 1) // 2))
+    if workers > 1:
+        import multiprocessing
+
+        with multiprocessing.get_context("spawn").Pool(workers) as pool:
+            pool.starmap(write_synthetic_artifact, jobs)
+    else:
+        for spec, path in jobs:
+            write_synthetic_artifact(spec, Path(path))
     return paths
 
 
@@ -828,7 +919,7 @@ def run_reference(args) -> None:
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{args.workload}", "k": k, "num_edges": E},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample, **host_info(workers)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))

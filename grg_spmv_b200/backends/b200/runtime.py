@@ -126,6 +126,9 @@ class B200PreparedMatmul:
         self._runtime._launch(self._args, self._graph)
 
 
+GPU_LIST_BUILD_MIN_EDGES = 1 << 21  # graphs at least this large build their level lists on the GPU
+
+
 class B200Runtime:
     """Runtime-owned B200 execution with resident or streamed level gather lists."""
 
@@ -288,17 +291,21 @@ class B200Runtime:
         coo = load_blocks(iter_artifact_blocks(art.path))
         levels = {}
         off = np.asarray(st.level_offsets, dtype=np.int64)
+        # Large graphs build their lists with PyTorch on the GPU (thousands of small launches,
+        # seconds saved at millions of edges); small ones with the NumPy builder, which gives
+        # identical lists and leaves the device to the traversal kernels.
+        list_device = self.device if int(art.scan.num_edges) >= GPU_LIST_BUILD_MIN_EDGES else None
         if up_on:
             plan = lay.pair.plan_up
             built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance,
-                                                            plan.pad_lists, plan.long_first, plan.slots, device=self.device)}
+                                                            plan.pad_lists, plan.long_first, plan.slots, device=list_device)}
             levels[Direction.UP] = self._upload_levels(art.levels_up, built)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
             plan = lay.pair.plan_down
             built = {lv.level: lv for lv in build_down_levels(
                 off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
-                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first, plan.slots, device=self.device)}
+                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first, plan.slots, device=list_device)}
             levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
         del coo
         return _DeviceArtifact(
