@@ -98,6 +98,8 @@ class _IntervalIndex:
         hi = self._search(base + cap.astype(np.int64), "right")
         hi = np.maximum(hi, lo + 1)  # the single-sample node (length 1) always qualifies
         uniform = lo + (rng.random(lo.size) * (hi - lo)).astype(np.int64)
+        if largest <= 0.0:  # uniform picks only (no second draw, so seeds give the same DAGs as before the option)
+            return self.ids[uniform]
         return self.ids[np.where(rng.random(lo.size) < largest, hi - 1, uniform)]
 
 

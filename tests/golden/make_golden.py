@@ -110,11 +110,12 @@ def _compare_states(ref_state, ours) -> None:
 
 SYNTH_CASES = {
     "synth_haploid": dict(num_samples=96, num_levels=6, num_nodes=700, num_mutations=160, children=(2, 8), random_ids=True, seed=11,
-                          neighbor_scale=0.5),
+                          neighbor_scale=0.5, prefer_largest=0.0),
     "synth_diploid": dict(num_samples=120, num_levels=7, num_nodes=900, num_mutations=200, children=(2, 6), ploidy=2,
-                          miss_fraction=0.05, with_coalescence=True, random_ids=True, seed=12, neighbor_scale=0.5),
+                          miss_fraction=0.05, with_coalescence=True, random_ids=True, seed=12, neighbor_scale=0.5,
+                          prefer_largest=0.0),
     "synth_repeat": dict(num_samples=64, num_levels=5, num_nodes=400, num_mutations=90, children=(2, 5), miss_fraction=0.1,
-                         random_ids=True, seed=13, neighbor_scale=0.5),
+                         random_ids=True, seed=13, neighbor_scale=0.5, prefer_largest=0.0),
 }
 
 

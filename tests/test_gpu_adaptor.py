@@ -1,6 +1,7 @@
 """Captured-graph adaptor (the reference's CapturedBoundGRG) on the B200 backend: results equal
-``BoundGRG.matmul``; k padding/truncation, int32 coercion, miss accumulation, native tensors
-and the reference's validation errors."""
+``BoundGRG.matmul`` and, for integer-valued inputs, the oracle bit for bit; k padding and
+truncation, int32 coercion, miss accumulation, native tensors and the reference's validation
+errors."""
 
 from __future__ import annotations
 
@@ -102,3 +103,49 @@ def test_captured_grg_validation_errors(artifact):
             cap.matmul(np.ones((2, S)), "up", emit_all_nodes=True)
         with pytest.raises(ValueError, match="Duplicate"):
             capture_grg(grg, None, req, stack, capture_ops=(CaptureSpec("up", 4), CaptureSpec("up", 4)))
+
+
+def test_captured_grg_matches_oracle_exactly_on_integer_inputs(artifact):
+    """The captured adaptor against the oracle (the reference's ReferenceRuntime arithmetic),
+    not against this backend's own eager path: integer-valued inputs are exact in FP64 in any
+    summation order, so every mode must agree bit for bit."""
+    from grg_oracle import OracleGRG
+
+    from grg_spmv_b200.adaptor import CaptureSpec, capture_grg
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+
+    req = _req()
+    layout = plan_b200_layout(artifacts=[str(artifact)], dtype=np.float64, requirements=req, vram_budget_bytes=0,
+                              ring_buffer_size=0, device=0, stream=0)
+    specs = (CaptureSpec("up", 6), CaptureSpec("down", 6), CaptureSpec("up", 6, by_individual=True),
+             CaptureSpec("down", 6, by_individual=True), CaptureSpec("down", 6, use_miss=True),
+             CaptureSpec("up", 6, use_miss=True), CaptureSpec("up", 6, init_mode="vector"),
+             CaptureSpec("down", 6, init_mode="matrix"), CaptureSpec("up", 6, init_mode="xtx"),
+             CaptureSpec("down", 6, init_mode="xtx"))
+    oracle = OracleGRG(str(artifact))
+    rng = np.random.default_rng(8)
+    ints = lambda shape, lo=-2, hi=3: rng.integers(lo, hi, size=shape).astype(np.float64)  # noqa: E731
+    with B200Runtime(layout, check_bounds=True) as runtime, contextlib.ExitStack() as stack:
+        (grg,) = runtime.grgs
+        cap = capture_grg(grg, None, req, stack, capture_ops=specs, native=False)
+        S, M, N, I = grg.num_samples, grg.num_mutations, grg.num_nodes, grg.num_individuals
+        for k in (6, 2):
+            x, xd, xi = ints((k, S)), ints((k, M)), ints((k, I))
+            np.testing.assert_array_equal(cap.matmul(x, "up"), oracle.matmul(x, "up"))
+            np.testing.assert_array_equal(cap.matmul(xd, "down"), oracle.matmul(xd, "down"))
+            np.testing.assert_array_equal(cap.matmul(xi, "up", by_individual=True), oracle.matmul(xi, "up", by_individual=True))
+            np.testing.assert_array_equal(cap.matmul(xd, "down", by_individual=True),
+                                          oracle.matmul(xd, "down", by_individual=True))
+            miss = ints((k, M), 0, 3)
+            np.testing.assert_array_equal(cap.matmul(xd, "down", miss=miss.copy()), oracle.matmul(xd, "down", miss=miss.copy()))
+            acc_cap = ints((k, M))
+            acc_ref = acc_cap.copy()
+            np.testing.assert_array_equal(cap.matmul(x, "up", miss=acc_cap), oracle.matmul(x, "up", miss=acc_ref))
+            np.testing.assert_array_equal(acc_cap, acc_ref)  # the up miss output accumulates in place
+            iv = ints(k)
+            np.testing.assert_array_equal(cap.matmul(x, "up", init=iv), oracle.matmul(x, "up", init=iv))
+            im = ints((k, N))
+            np.testing.assert_array_equal(cap.matmul(xd, "down", init=im), oracle.matmul(xd, "down", init=im))
+            np.testing.assert_array_equal(cap.matmul(x, "up", init="xtx"), oracle.matmul(x, "up", init="xtx"))
+            np.testing.assert_array_equal(cap.matmul(xd, "down", init="xtx"), oracle.matmul(xd, "down", init="xtx"))
+        assert runtime.device_error() == 0
