@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 12
+ABI_VERSION = 13
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -142,6 +142,36 @@ class TraverseArgs(ctypes.Structure):
     ]
 
 
+class RowopArgs(ctypes.Structure):
+    _fields_ = [
+        ("rows", ctypes.c_int64),
+        ("k", ctypes.c_int64),
+        ("ld", ctypes.c_int64),
+        ("src", ctypes.c_void_p),
+        ("dst", ctypes.c_void_p),
+        ("miss_in", ctypes.c_void_p),
+        ("miss_scale", ctypes.c_void_p),
+        ("pre_scale", ctypes.c_void_p),
+        ("col_sub", ctypes.c_void_p),
+        ("sub_scale", ctypes.c_void_p),
+        ("post_scale", ctypes.c_void_p),
+        ("miss_out", ctypes.c_void_p),
+        ("miss_out_scale", ctypes.c_void_p),
+        ("col_sums", ctypes.c_int32),
+        ("sum_weight", ctypes.c_void_p),
+        ("partials", ctypes.c_void_p),
+        ("sums", ctypes.c_void_p),
+    ]
+
+
+ROWOP_MAX_BLOCKS = 1184
+
+
+def rowop_blocks(rows: int) -> int:
+    """GRG_B200_ROWOP_BLOCKS: row blocks (and rows of partial sums) of a rowop call."""
+    return min((int(rows) + 255) // 256, ROWOP_MAX_BLOCKS)
+
+
 EXPORTED_SYMBOLS = (
     "grg_b200_abi_version",
     "grg_b200_last_error",
@@ -154,6 +184,7 @@ EXPORTED_SYMBOLS = (
     "grg_b200_emit_all",
     "grg_b200_traverse",
     "grg_b200_traverse_static",
+    "grg_b200_rowop",
 )
 
 _lock = threading.Lock()
@@ -198,6 +229,8 @@ def load_library():
                      "grg_b200_traverse_static"):
             getattr(lib, name).argtypes = [ctypes.POINTER(TraverseArgs), ctypes.c_void_p]
             getattr(lib, name).restype = ctypes.c_int
+        lib.grg_b200_rowop.argtypes = [ctypes.POINTER(RowopArgs), ctypes.c_void_p]
+        lib.grg_b200_rowop.restype = ctypes.c_int
         lib.grg_b200_run_level.argtypes = [ctypes.POINTER(TraverseArgs), ctypes.POINTER(Level), ctypes.c_void_p]
         lib.grg_b200_run_level.restype = ctypes.c_int
         version = int(lib.grg_b200_abi_version())
@@ -222,6 +255,7 @@ __all__ = [
     "EXPORTED_SYMBOLS",
     "LIB_PATH",
     "Level",
+    "RowopArgs",
     "TraverseArgs",
     "build_library",
     "check",

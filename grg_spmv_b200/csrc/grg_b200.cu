@@ -2551,6 +2551,72 @@ int encode_down_inputs(const grg_b200_traverse_args* a, const Shape& sh, cudaStr
 
 }  // namespace
 
+// ---------------------------------------------------------------------------------------
+// Standardised-operator row step (grg_b200_rowop): one pass over a [rows, k] buffer applying
+// the per-row affine map of the header, with deterministic column sums.  A block owns
+// GRG_B200_ROWOP_ROWS_PER_BLOCK consecutive rows; its 256 threads form ny = 256 / kt row
+// groups of kt column lanes (kt: k rounded up to a power of two, at most 256).  Lane (x, y)
+// walks rows y, y + ny, ... of the block for column c0 + x, so a warp reads contiguous
+// columns of a row; the ny partial sums are added in y order, and the finalize kernel adds
+// the blocks' partials in block order.
+// ---------------------------------------------------------------------------------------
+constexpr int kRowopThreads = 256;
+
+__global__ void __launch_bounds__(kRowopThreads) rowop_kernel(grg_b200_rowop_args a, int log2kt, int64_t rows_per_block) {
+    __shared__ double red[kRowopThreads];
+    const int kt = 1 << log2kt;
+    const int tx = threadIdx.x & (kt - 1);
+    const int ty = threadIdx.x >> log2kt;
+    const int ny = kRowopThreads >> log2kt;
+    const int64_t r0 = static_cast<int64_t>(blockIdx.x) * rows_per_block;
+    const int64_t r1 = r0 + rows_per_block < a.rows ? r0 + rows_per_block : a.rows;
+    for (int64_t c0 = 0; c0 < a.k; c0 += kt) {
+        const int64_t j = c0 + tx;
+        const bool active = j < a.k;
+        const double cs = active && a.col_sub ? __ldg(a.col_sub + j) : 0.0;
+        double part = 0.0;
+        if (active) {
+            for (int64_t r = r0 + ty; r < r1; r += ny) {
+                const int64_t e = r * a.ld + j;
+                double t = __ldg(a.src + e);
+                if (a.miss_in) t = __dadd_rn(t, __dmul_rn(__ldg(a.miss_in + e), __ldg(a.miss_scale + r)));
+                if (a.pre_scale) t = __dmul_rn(t, __ldg(a.pre_scale + r));
+                if (a.col_sub) t = __dsub_rn(t, a.sub_scale ? __dmul_rn(cs, __ldg(a.sub_scale + r)) : cs);
+                if (a.post_scale) t = __dmul_rn(t, __ldg(a.post_scale + r));
+                a.dst[e] = t;
+                if (a.miss_out) a.miss_out[e] = __dmul_rn(t, __ldg(a.miss_out_scale + r));
+                if (a.col_sums) part = __dadd_rn(part, a.sum_weight ? __dmul_rn(t, __ldg(a.sum_weight + r)) : t);
+            }
+        }
+        if (a.col_sums) {  // uniform across the block
+            red[threadIdx.x] = part;
+            __syncthreads();
+            if (ty == 0 && active) {
+                double s = red[tx];
+                for (int y = 1; y < ny; ++y) s = __dadd_rn(s, red[(y << log2kt) + tx]);
+                a.partials[static_cast<int64_t>(blockIdx.x) * a.k + j] = s;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// One CTA per column: thread t adds the partials of blocks t, t + 256, ... in order, then a
+// fixed tree combines the 256 sums.
+__global__ void __launch_bounds__(256) rowop_finalize_kernel(const double* partials, int64_t blocks, int64_t k, double* sums) {
+    __shared__ double red[256];
+    const int64_t j = blockIdx.x;
+    double s = 0.0;
+    for (int64_t b = threadIdx.x; b < blocks; b += 256) s = __dadd_rn(s, partials[b * k + j]);
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (static_cast<int>(threadIdx.x) < w) red[threadIdx.x] = __dadd_rn(red[threadIdx.x], red[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) sums[j] = red[0];
+}
+
 struct grg_b200_ring {
     int device;
     int num_slots;
@@ -2564,6 +2630,32 @@ struct grg_b200_ring {
 extern "C" {
 
 int grg_b200_abi_version(void) { return GRG_B200_ABI_VERSION; }
+
+int grg_b200_rowop(const grg_b200_rowop_args* a, void* stream_handle) {
+    if (!a) return fail(GRG_B200_ERR_INVALID, "args is NULL");
+    if (a->rows < 0 || a->k < 1 || a->ld < a->k)
+        return fail(GRG_B200_ERR_INVALID, "rowop needs rows >= 0, k >= 1 and ld >= k (got %lld, %lld, %lld)",
+                    (long long)a->rows, (long long)a->k, (long long)a->ld);
+    if (!a->src || !a->dst) return fail(GRG_B200_ERR_INVALID, "rowop src/dst is NULL");
+    if (a->miss_in && !a->miss_scale) return fail(GRG_B200_ERR_INVALID, "rowop miss_in needs miss_scale");
+    if (a->miss_out && !a->miss_out_scale) return fail(GRG_B200_ERR_INVALID, "rowop miss_out needs miss_out_scale");
+    if (a->col_sums && (!a->partials || !a->sums)) return fail(GRG_B200_ERR_INVALID, "rowop col_sums needs partials and sums");
+    if (a->rows == 0) return GRG_B200_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream_handle);
+    int log2kt = 0;
+    while ((int64_t{1} << log2kt) < a->k && log2kt < 8) ++log2kt;
+    const int64_t blocks = GRG_B200_ROWOP_BLOCKS(a->rows);
+    const int64_t rows_per_block = (a->rows + blocks - 1) / blocks;
+    if (a->k > 0x7fffffff) return fail(GRG_B200_ERR_UNSUPPORTED, "rowop: k = %lld is too large", (long long)a->k);
+    rowop_kernel<<<dim3(static_cast<unsigned>(blocks)), kRowopThreads, 0, s>>>(*a, log2kt, rows_per_block);
+    GRG_LAUNCH_CHECK("rowop_kernel");
+    if (a->col_sums) {
+        rowop_finalize_kernel<<<dim3(static_cast<unsigned>(a->k)), 256, 0, s>>>(a->partials, blocks, a->k, a->sums);
+        GRG_LAUNCH_CHECK("rowop_finalize_kernel");
+    }
+    return GRG_B200_OK;
+}
+
 
 size_t grg_b200_last_error(char* buf, size_t buf_size) {
     const size_t n = strlen(g_last_error);

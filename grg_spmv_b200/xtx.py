@@ -12,9 +12,12 @@ centring folded in as rank-one corrections (``_body``, ``:326-347``):
     u   = down(d) - c_down               c_up = row sums of u
     out = (up(u) (+ p * up_miss)) / sigma - c_up * centre / sigma
 
-Everything outside the two traversals is FP64 elementwise work on the runtime's stream (the
-reference does it with CuPy); the traversals are the B200 kernels, in plain FP64 or in the
-mixed precision of the runtime's layout.  ``randomized_eigh`` is the reference's
+Everything outside the two traversals is FP64 work on the runtime's stream, fused into one
+library pass per step (``grg_b200_rowop``: the per-row scaling, the miss rows, the centring and
+the deterministic column sums that replace the reference's CuPy elementwise chain, its cuBLAS
+``d @ centre`` and its ``row_weighted_sum`` kernel, ``:32-61``).  One application is three such
+passes around the two traversals; the traversals are the B200 kernels, in plain FP64 or in
+the mixed precision of the runtime's layout.  ``randomized_eigh`` is the reference's
 randomized Rayleigh-Ritz solver (``_run_randomized_rr``, ``:656-669``) with FP64 QR and eigh.
 
 ``StandardizedXXT`` is the individual-space counterpart ``Z Zᵀ`` (the kinship product of the
@@ -25,6 +28,34 @@ FP64 dot products and residuals.
 """
 
 from __future__ import annotations
+
+import ctypes
+
+from grg_spmv_b200.backends.b200 import _native as nat
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else int(t.data_ptr())
+
+
+class _RowStep:
+    """One ``grg_b200_rowop`` pass with fixed buffers (the source may change per call)."""
+
+    def __init__(self, lib, stream_ptr: int, *, rows: int, k: int, src=None, dst, miss_in=None, miss_scale=None,
+                 pre_scale=None, col_sub=None, sub_scale=None, post_scale=None, miss_out=None, miss_out_scale=None,
+                 sums=None, sum_weight=None, partials=None) -> None:
+        self._lib = lib
+        self._stream = ctypes.c_void_p(stream_ptr)
+        self.args = nat.RowopArgs(rows=int(rows), k=int(k), ld=int(k), src=_ptr(src), dst=_ptr(dst), miss_in=_ptr(miss_in),
+                                  miss_scale=_ptr(miss_scale), pre_scale=_ptr(pre_scale), col_sub=_ptr(col_sub),
+                                  sub_scale=_ptr(sub_scale), post_scale=_ptr(post_scale), miss_out=_ptr(miss_out),
+                                  miss_out_scale=_ptr(miss_out_scale), col_sums=int(sums is not None),
+                                  sum_weight=_ptr(sum_weight), partials=_ptr(partials), sums=_ptr(sums))
+
+    def __call__(self, src=None) -> None:
+        if src is not None:
+            self.args.src = int(src.data_ptr())
+        nat.check(self._lib, self._lib.grg_b200_rowop(ctypes.byref(self.args), self._stream), "grg_b200_rowop")
 
 
 class StandardizedXTX:
@@ -60,6 +91,23 @@ class StandardizedXTX:
             self._down = grg.prepare_matmul_cuda(direction="down", k=self.q, by_individual=True, use_miss=self.has_missing)
             self._up = grg.prepare_matmul_cuda(direction="up", k=self.q, by_individual=True, use_miss=self.has_missing)
             self._out = torch.empty((self.shape[0], self.q), device=dev, dtype=torch.float64)
+            M, I = int(grg.num_mutations), int(grg.num_individuals)
+            self._partials = torch.empty((nat.rowop_blocks(max(M, I)), self.q), device=dev, dtype=torch.float64)
+            self.c_down = torch.empty(self.q, device=dev, dtype=torch.float64)
+            self.c_up = torch.empty(self.q, device=dev, dtype=torch.float64)
+        lib, sp = runtime._lib, int(self._stream.cuda_stream)
+        down, up, miss = self._down, self._up, self.has_missing
+        # d = v / sigma (and its miss rows d * p), c_down = d . centre
+        self._encode = _RowStep(lib, sp, rows=M, k=self.q, dst=down.input, pre_scale=self.inv_sigma,
+                                miss_out=down.miss_input if miss else None, miss_out_scale=self.freqs if miss else None,
+                                sums=self.c_down, sum_weight=self.center, partials=self._partials)
+        # u = down(d) - c_down in place (it is up's input), c_up = column sums of u
+        self._center = _RowStep(lib, sp, rows=I, k=self.q, src=down.output, dst=up.input, col_sub=self.c_down,
+                                sums=self.c_up, partials=self._partials)
+        # out = (up(u) + p * up_miss) / sigma - c_up * centre / sigma
+        self._finish = _RowStep(lib, sp, rows=M, k=self.q, src=up.output, dst=self._out,
+                                miss_in=up.miss_output if miss else None, miss_scale=self.freqs if miss else None,
+                                pre_scale=self.inv_sigma, col_sub=self.c_up, sub_scale=self.center_over_sigma)
 
     def apply(self, v):
         """``Zᵀ Z v`` for ``v`` of shape ``(M, q)`` (a CUDA FP64 tensor); returns a new ``(M, q)`` tensor."""
@@ -67,24 +115,15 @@ class StandardizedXTX:
 
         if tuple(v.shape) != (self.shape[0], self.q):
             raise ValueError(f"operand has shape {tuple(v.shape)}, expected ({self.shape[0]}, {self.q})")
-        down, up = self._down, self._up
+        if v.dtype != torch.float64 or v.device != self._out.device:
+            raise ValueError("operand must be a float64 tensor on the runtime's device")
         with torch.cuda.stream(self._stream):
-            torch.mul(v.T, self.inv_sigma[None, :], out=down.input)
-            if self.has_missing:
-                torch.mul(down.input, self.freqs[None, :], out=down.miss_input)
-            c_down = down.input @ self.center
-            down()
-            u = down.output - c_down[:, None]
-            c_up = u.sum(dim=1)
-            up.input.copy_(u)
-            if self.has_missing:
-                up.miss_output.fill_(0.0)
-            up()
-            res = up.output
-            if self.has_missing:
-                res = res + up.miss_output * self.freqs[None, :]
-            res = res * self.inv_sigma[None, :] - c_up[:, None] * self.center_over_sigma[None, :]
-            self._out.copy_(res.T)
+            v = v.contiguous()
+            self._encode(v)
+            self._down()
+            self._center()
+            self._up()
+            self._finish()
             return self._out.clone()
 
 
@@ -100,6 +139,21 @@ class StandardizedXXT:
         self.q = int(q)
         self.shape = (int(grg.num_individuals), int(grg.num_individuals))
         self._out = torch.empty(self.shape[0], self.q, device=self._xtx._out.device, dtype=torch.float64)
+        x = self._xtx
+        lib, sp = runtime._lib, int(x._stream.cuda_stream)
+        down, up, miss = x._down, x._up, x.has_missing
+        M, I = int(grg.num_mutations), int(grg.num_individuals)
+        # up's input = w, c_up = column sums of w
+        self._load = _RowStep(lib, sp, rows=I, k=self.q, dst=up.input, sums=x.c_up, partials=x._partials)
+        # t = (up(w) + p * up_miss) / sigma - c_up * centre / sigma; down's input d = t / sigma,
+        # its miss rows d * p, c_down = d . centre
+        self._mid = _RowStep(lib, sp, rows=M, k=self.q, src=up.output, dst=down.input,
+                             miss_in=up.miss_output if miss else None, miss_scale=x.freqs if miss else None,
+                             pre_scale=x.inv_sigma, col_sub=x.c_up, sub_scale=x.center_over_sigma, post_scale=x.inv_sigma,
+                             miss_out=down.miss_input if miss else None, miss_out_scale=x.freqs if miss else None,
+                             sums=x.c_down, sum_weight=x.center, partials=x._partials)
+        # out = down(d) - c_down
+        self._finish = _RowStep(lib, sp, rows=I, k=self.q, src=down.output, dst=self._out, col_sub=x.c_down)
 
     def apply(self, w):
         import torch
@@ -107,23 +161,15 @@ class StandardizedXXT:
         x = self._xtx
         if tuple(w.shape) != (self.shape[0], self.q):
             raise ValueError(f"operand has shape {tuple(w.shape)}, expected ({self.shape[0]}, {self.q})")
-        down, up = x._down, x._up
+        if w.dtype != torch.float64 or w.device != self._out.device:
+            raise ValueError("operand must be a float64 tensor on the runtime's device")
         with torch.cuda.stream(x._stream):
-            up.input.copy_(w.T)  # Zᵀ w
-            c_up = up.input.sum(dim=1)
-            if x.has_missing:
-                up.miss_output.fill_(0.0)
-            up()
-            t = up.output.clone()
-            if x.has_missing:
-                t += up.miss_output * x.freqs[None, :]
-            t = t * x.inv_sigma[None, :] - c_up[:, None] * x.center_over_sigma[None, :]
-            torch.mul(t, x.inv_sigma[None, :], out=down.input)  # Z t
-            if x.has_missing:
-                torch.mul(down.input, x.freqs[None, :], out=down.miss_input)
-            c_down = down.input @ x.center
-            down()
-            self._out.copy_((down.output - c_down[:, None]).T)
+            w = w.contiguous()
+            self._load(w)
+            x._up()
+            self._mid()
+            x._down()
+            self._finish()
             return self._out.clone()
 
 

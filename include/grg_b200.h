@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 12
+#define GRG_B200_ABI_VERSION 13
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -296,6 +296,53 @@ int grg_b200_emit_all(const grg_b200_traverse_args* args, void* stream);
 /* The full prepared call: seed, every level (copying streamed levels through the ring), and
  * the output stage, all on `stream`. */
 int grg_b200_traverse(const grg_b200_traverse_args* args, void* stream);
+
+/*
+ * Row-wise step of the standardised genotype Gram operators (Z^T Z and Z Z^T with Z centred by
+ * the allele mean and scaled by 1/sigma per mutation): the FP64 work between and after the two
+ * traversals, fused into one pass over a [rows, k] buffer (row stride ld for every buffer).
+ * Replaces the CuPy/cuBLAS steps of the reference's PreparedXTX._body
+ * (scripts/pca_bench/__main__.py:326-347) and its row_weighted_sum kernel (:32-61), and the
+ * kinship product of scripts/bolt_lmm_inf/core.py:1241-1301.  Per row r and column j:
+ *     t = src[r, j]
+ *     if miss_in:    t = t + miss_in[r, j] * miss_scale[r]
+ *     if pre_scale:  t = t * pre_scale[r]
+ *     if col_sub:    t = t - col_sub[j] * (sub_scale ? sub_scale[r] : 1)
+ *     if post_scale: t = t * post_scale[r]
+ *     dst[r, j] = t;  if miss_out: miss_out[r, j] = t * miss_out_scale[r]
+ *     if col_sums:   sums[j] = sum over r of t * (sum_weight ? sum_weight[r] : 1)
+ * Every product and sum is rounded separately (no fused multiply-add).  The column sums are
+ * deterministic: fixed row blocks, a fixed in-block order, then the blocks' partials in block
+ * order (partials needs GRG_B200_ROWOP_BLOCKS(rows) * k doubles, each row block a contiguous
+ * range of ceil(rows / blocks) rows).  src may equal dst and
+ * miss_in may equal miss_out (each element is read before it is written, by one thread).
+ */
+typedef struct grg_b200_rowop_args {
+    int64_t rows;
+    int64_t k;
+    int64_t ld;
+    const double* src;
+    double* dst;
+    const double* miss_in;
+    const double* miss_scale;
+    const double* pre_scale;
+    const double* col_sub;
+    const double* sub_scale;
+    const double* post_scale;
+    double* miss_out;
+    const double* miss_out_scale;
+    int32_t col_sums;
+    const double* sum_weight;
+    double* partials;
+    double* sums;
+} grg_b200_rowop_args;
+
+/* Row blocks of a rowop call: one per 256 rows, at most 1184 (the partial sums hold one row of
+ * k doubles per block). */
+#define GRG_B200_ROWOP_MAX_BLOCKS 1184
+#define GRG_B200_ROWOP_BLOCKS(rows) \
+    ((((rows) + 255) / 256) < GRG_B200_ROWOP_MAX_BLOCKS ? (((rows) + 255) / 256) : GRG_B200_ROWOP_MAX_BLOCKS)
+int grg_b200_rowop(const grg_b200_rowop_args* args, void* stream);
 
 /* No counterpart in the reference.  The same traversal as grg_b200_traverse for callers that
  * cannot allocate device memory (C/FFI hosts without a device allocator, plugins inside
