@@ -641,6 +641,7 @@ def run_b200(args) -> None:
         config_blocks = [int(b) for b in args.tier_blocks.split(",") if b]
         tiers = {"single_graph": measure_tiers(args, [path], device, stream, [config_blocks])[0]}
         torch.cuda.empty_cache()
+        tiers["pca_operator"] = measure_xtx_operator(path, device)
         if args.tier_grgs > 0:
             t0 = time.perf_counter()
             multi = make_multi_artifacts(args)
@@ -701,6 +702,45 @@ def run_b200(args) -> None:
         print(json.dumps(line))
     if world > 1:
         dist.destroy_process_group()
+
+
+def measure_xtx_operator(path, device, q: int = 64, applies: int = 5) -> dict:
+    """The standardised Gram operator Zᵀ Z (randomized PCA's operator) at block width ``q`` on
+    ``path``: device time per application (one down and one up traversal by individual plus
+    the three fused FP64 passes around them), CUDA events on the runtime's stream."""
+    import torch
+
+    from grg_spmv_b200 import RuntimeRequirements, scan_grg_spmv
+    from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
+    from grg_spmv_b200.xtx import StandardizedXTX
+
+    scan = scan_grg_spmv(path)
+    req = RuntimeRequirements(max_k_up=q, max_k_down=q, need_down_miss_input=scan.has_missing_data,
+                              need_up_miss_output=scan.has_missing_data, need_init_vector=False, need_init_matrix=False,
+                              need_init_xtx=False)
+    stream = torch.cuda.Stream(device=device)
+    layout = plan_b200_layout(artifacts=[path], dtype=np.float64, requirements=req, vram_budget_bytes=0, ring_buffer_size=0,
+                              device=device.index or 0, stream=stream, emit_all_nodes=False)
+    with B200Runtime(layout) as rt, torch.cuda.stream(stream):
+        (grg,) = rt.grgs
+        op = StandardizedXTX(rt, grg, q)
+        v = torch.randn((grg.num_mutations, q), dtype=torch.float64, device=device, generator=torch.Generator(device=device).manual_seed(5))
+        for _ in range(2):
+            op.apply(v)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(applies):
+            v = op.apply(v)
+            v = v / torch.linalg.vector_norm(v, dim=0, keepdim=True)
+        b.record(stream)
+        torch.cuda.synchronize(device)
+        ms = a.elapsed_time(b) / applies
+    del op, rt
+    torch.cuda.empty_cache()
+    return {"q": q, "applications": applies, "ms_per_application": ms,
+            "edge_rhs_per_s": 2.0 * scan.num_edges * q / (ms / 1e3),
+            "note": "each application: fused encode pass, down traversal, fused centring pass, up traversal, fused "
+                    "finish pass (plus the harness's column normalisation between applications)"}
 
 
 def multi_grg_specs(count: int, scale: float):
