@@ -94,8 +94,6 @@ def parse_args():
     p.add_argument("--narrow-split", type=int, default=None, help="narrow rows split over 2^n lane groups (-1: per level)")
     p.add_argument("--fuse-entries", type=int, default=None,
                    help="run stretches of levels with at most this many entries as one cooperative launch (0: off)")
-    p.add_argument("--cache-hints", choices=["none", "lists", "inputs", "both"], default=None,
-                   help="L2 evict_first hints on loads of read-once data (default: the plan's)")
     p.add_argument("--schedule", choices=["levels", "dataflow"], default=None,
                    help="one launch per level, or one persistent dataflow launch per traversal")
     p.add_argument("--precision", choices=["plain", "mixed"], default="plain",
@@ -319,8 +317,6 @@ def run_b200(args) -> None:
         extra["fuse_entries"] = args.fuse_entries
     if args.schedule is not None:
         extra["schedule"] = args.schedule
-    if args.cache_hints is not None:
-        extra["cache_hints"] = args.cache_hints
     pair = B200PlanPair(plan_up=B200Plan(exact_order=args.exact_order, row_order=args.row_order_up,
                                          slots=args.slots in ("up", "both"), **extra),
                         plan_down=B200Plan(exact_order=args.exact_order, row_order=args.row_order_down,
@@ -673,7 +669,7 @@ def run_b200(args) -> None:
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
                        "long_first": pair.plan_down.long_first, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
-                       "schedule": pair.plan_down.schedule, "cache_hints": pair.plan_down.cache_hints,
+                       "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",
                                      "down": "locality" if pair.plan_down.locality(Direction.DOWN) else "natural"},

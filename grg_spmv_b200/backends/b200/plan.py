@@ -31,7 +31,6 @@ import warnings
 import numpy as np
 
 from grg_spmv_b200.artifact import ArtifactScan, scan_grg_spmv
-from grg_spmv_b200.backends.b200 import _native as nat
 from grg_spmv_b200.backends.b200.structures import blob_layout, down_entry_bound, up_entry_bound
 from grg_spmv_b200.types import Direction
 
@@ -87,9 +86,6 @@ class B200Plan:
     lists, plain precision; other calls fall back to "levels").
     ``persist_ctas``: with ``narrow_variant`` 9 or 10, the CTAs of a level launch's persistent
     narrow part (each walks row groups); 0 sizes it to what the GPU holds at once.
-    ``cache_hints``: L2 eviction-priority hints on loads of data a traversal reads once:
-    "lists" (row pointers, row ids and gather codes), "inputs" (down input and miss rows),
-    "both" or "none".  The hints are per load instruction and change no cache setting.
     ``fuse_entries``: > 0 runs each stretch of consecutive resident levels with at most this many
     gather entries (default mode, plain precision, padded variants) as one cooperative launch
     with a grid barrier between levels instead of one launch per level; results are
@@ -111,7 +107,6 @@ class B200Plan:
     schedule: str = "levels"
     persist_ctas: int = 0
     fuse_entries: int = 0
-    cache_hints: str = "none"
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -132,17 +127,6 @@ class B200Plan:
             raise ValueError(f"persist_ctas must be >= 0, got {self.persist_ctas}")
         if int(self.fuse_entries) < 0:
             raise ValueError(f"fuse_entries must be >= 0, got {self.fuse_entries}")
-        if self.cache_hints not in ("none", "lists", "inputs", "both"):
-            raise ValueError(f"cache_hints must be 'none', 'lists', 'inputs' or 'both', got {self.cache_hints!r}")
-
-    def launch_hint_flags(self) -> int:
-        """The GRG_B200_LAUNCH_*_EVICT_FIRST bits of ``cache_hints``."""
-        flags = 0
-        if self.cache_hints in ("lists", "both"):
-            flags |= nat.LAUNCH_LISTS_EVICT_FIRST
-        if self.cache_hints in ("inputs", "both"):
-            flags |= nat.LAUNCH_INPUTS_EVICT_FIRST
-        return flags
 
     def resolve_narrow_variant(self, k: int) -> int:
         """The narrow-row kernel variant used for a call with ``k`` right-hand sides."""

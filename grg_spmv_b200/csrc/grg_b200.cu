@@ -157,43 +157,12 @@ __device__ __forceinline__ Pack<T, V> ld_l2(const T* p) {
     return r;
 }
 
-// L2 eviction-priority hints: data read once (level lists, down input rows) is loaded with an
-// evict_first policy so that it leaves L2 before node rows that later levels read again.
-__device__ __forceinline__ uint64_t evict_first_policy() {
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-
 // Source-row load of the level walkers: the read-only path, or L2 only (CG) where rows read
 // here may have been written by other SMs earlier in the same launch.
 template <typename T, int V, bool CG>
 __device__ __forceinline__ Pack<T, V> ld_src(const T* p) {
     if constexpr (CG) return ld_l2<T, V>(p);
     else return ld_ro<T, V>(p);
-}
-
-// Read-only load with an L2 evict_first policy (rows read once per traversal).
-template <typename T, int V>
-__device__ __forceinline__ Pack<T, V> ld_once(const T* p) {
-    Pack<T, V> r;
-    const uint64_t pol = evict_first_policy();
-    if constexpr (std::is_same<T, double>::value && V == 2) {
-        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
-                     : "=d"(r.v[0]), "=d"(r.v[1]) : "l"(p), "l"(pol));
-    } else if constexpr (std::is_same<T, double>::value && V == 1) {
-        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(r.v[0]) : "l"(p), "l"(pol));
-    } else if constexpr (std::is_same<T, float>::value && V == 4) {
-        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-                     : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]) : "l"(p), "l"(pol));
-    } else if constexpr (std::is_same<T, float>::value && V == 2) {
-        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f32 {%0, %1}, [%2], %3;"
-                     : "=f"(r.v[0]), "=f"(r.v[1]) : "l"(p), "l"(pol));
-    } else {
-        static_assert(std::is_same<T, float>::value && V == 1, "unsupported pack");
-        asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(r.v[0]) : "l"(p), "l"(pol));
-    }
-    return r;
 }
 
 template <typename T, int V>
@@ -246,36 +215,7 @@ struct LevelArgs {
     void* state_lo;
     const void* x_lo;
     const void* miss_lo;
-    int32_t list_hint;   // level lists loaded with L2 evict_first (GRG_B200_LAUNCH_LISTS_EVICT_FIRST)
-    int32_t input_hint;  // down input/miss rows loaded with L2 evict_first (GRG_B200_LAUNCH_INPUTS_EVICT_FIRST)
 };
-
-
-__device__ __forceinline__ uint4 ld_list4(const LevelArgs& a, const uint4* p) {
-    if (!a.list_hint) return __ldg(p);
-    uint4 v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
-                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
-                 : "l"(p), "l"(evict_first_policy()));
-    return v;
-}
-
-template <typename I>
-__device__ __forceinline__ I ld_list(const LevelArgs& a, const I* p) {
-    static_assert(sizeof(I) == 4, "32-bit list words");
-    if (!a.list_hint) return __ldg(p);
-    uint32_t v;
-    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(evict_first_policy()));
-    return static_cast<I>(v);
-}
-
-// A gather entry's source row: input and miss rows (read once per traversal) take the
-// evict_first path when the launch asks for it, state rows the normal read-only path.
-template <typename T, int V, bool CG>
-__device__ __forceinline__ Pack<T, V> ld_entry(const LevelArgs& a, uint32_t code, const T* p) {
-    if (a.input_hint && ((code >> GRG_B200_SRC_SHIFT) & GRG_B200_SRC_MASK) != GRG_B200_SRC_STATE) return ld_once<T, V>(p);
-    return ld_src<T, V, CG>(p);
-}
 
 enum DeviceError : int32_t {
     kErrStateId = 1,
@@ -352,7 +292,7 @@ constexpr int kStageCap = 1024;  // gather-list entries staged in shared memory 
 constexpr unsigned kFullMask = 0xffffffffu;
 
 __device__ __forceinline__ int64_t level_row(const LevelArgs& a, int64_t pos) {
-    return a.row_begin + (a.row_ids ? static_cast<int64_t>(ld_list(a, a.row_ids + pos)) : pos);
+    return a.row_begin + (a.row_ids ? static_cast<int64_t>(__ldg(a.row_ids + pos)) : pos);
 }
 
 // Narrow rows.  A warp owns 32/G consecutive processing positions; lane group g (G lanes)
@@ -540,8 +480,8 @@ __device__ __forceinline__ void narrow_extent(const LevelArgs& a, int64_t pos, i
         e0 = static_cast<int32_t>(a.slot_entry[b] + (pos - a.slot_pos[b]) * w);
         e1 = e0 + w;
     } else {
-        e0 = ld_list(a, a.row_ptr + pos);
-        e1 = ld_list(a, a.row_ptr + pos + 1);
+        e0 = __ldg(a.row_ptr + pos);
+        e1 = __ldg(a.row_ptr + pos + 1);
     }
 }
 
@@ -561,7 +501,7 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
     uint4 first[Q];  // the list is static: fetched before waiting for the previous level
 #pragma unroll
-    for (int j = 0; j < Q; ++j) first[j] = (e0 >> 2) + j < (e1 >> 2) ? ld_list4(a, codes4 + (e0 >> 2) + j) : null4;
+    for (int j = 0; j < Q; ++j) first[j] = (e0 >> 2) + j < (e1 >> 2) ? __ldg(codes4 + (e0 >> 2) + j) : null4;
     pdl_wait();
     T* state = static_cast<T*>(a.state);
     const int64_t step = static_cast<int64_t>(V) << a.log2g;
@@ -576,7 +516,7 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
         for (; q < q1; q += Q) {  // Q quads (4 * Q row fetches) in flight per round
             uint4 nxt[Q];
 #pragma unroll
-            for (int j = 0; j < Q; ++j) nxt[j] = q + Q + j < q1 ? ld_list4(a, codes4 + q + Q + j) : null4;
+            for (int j = 0; j < Q; ++j) nxt[j] = q + Q + j < q1 ? __ldg(codes4 + q + Q + j) : null4;
             uint32_t code[4 * Q];
 #pragma unroll
             for (int j = 0; j < Q; ++j) {
@@ -591,7 +531,7 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
             for (int u = 0; u < 4 * Q; ++u) {
                 const T* src = entry_row<T>(a, code[u]);
                 valid[u] = src != nullptr;
-                val[u] = valid[u] ? ld_entry<T, V, CG>(a, code[u], src + c) : zero_pack<T, V>();
+                val[u] = valid[u] ? ld_src<T, V, CG>(src + c) : zero_pack<T, V>();
             }
 #pragma unroll
             for (int u = 0; u < 4 * Q; ++u) {
@@ -632,8 +572,8 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
     int32_t e0 = 0, e1 = 0;
     int64_t row = 0;
     if (live) {
-        e0 = ld_list(a, a.row_ptr + pos);
-        e1 = ld_list(a, a.row_ptr + pos + 1);
+        e0 = __ldg(a.row_ptr + pos);
+        e1 = __ldg(a.row_ptr + pos + 1);
         row = level_row(a, pos);
     }
     pdl_wait();
@@ -646,13 +586,13 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
         Pack<T, V> part = zero_pack<T, V>();
         if (live) {
             for (int32_t q = (e0 >> 2) + sub; q < (e1 >> 2); q += 1 << a.log2s) {
-                const uint4 cq = ld_list4(a, codes4 + q);
+                const uint4 cq = __ldg(codes4 + q);
                 const uint32_t code[4] = {cq.x, cq.y, cq.z, cq.w};
                 Pack<T, V> val[4];
 #pragma unroll
                 for (int u = 0; u < 4; ++u) {
                     const T* src = entry_row<T>(a, code[u]);
-                    val[u] = src ? ld_entry<T, V, false>(a, code[u], src + c) : zero_pack<T, V>();
+                    val[u] = src ? ld_ro<T, V>(src + c) : zero_pack<T, V>();
                 }
 #pragma unroll
                 for (int u = 0; u < 4; ++u) add_into(part, val[u]);
@@ -692,9 +632,9 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
     const int64_t w = block * WPC + (threadIdx.x >> 5);
     if (w >= a.num_heavy) return;  // warp-uniform
     const int lane32 = threadIdx.x & 31;
-    const int64_t pos = ld_list(a, a.heavy_rows + w);
-    const int32_t e0 = ld_list(a, a.row_ptr + pos);
-    const int32_t e1 = ld_list(a, a.row_ptr + pos + 1);
+    const int64_t pos = __ldg(a.heavy_rows + w);
+    const int32_t e0 = __ldg(a.row_ptr + pos);
+    const int32_t e1 = __ldg(a.row_ptr + pos + 1);
     const int64_t row = level_row(a, pos);
     pdl_wait();
     const int g_lanes = 1 << a.log2g;
@@ -716,15 +656,15 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
                 const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
                 const int32_t q1 = e1 >> 2;
                 int32_t q = (e0 >> 2) + grp;
-                uint4 cur = q < q1 ? ld_list4(a, codes4 + q) : null4;
+                uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
                 for (; q < q1; q += groups) {
-                    const uint4 nxt = q + groups < q1 ? ld_list4(a, codes4 + q + groups) : null4;
+                    const uint4 nxt = q + groups < q1 ? __ldg(codes4 + q + groups) : null4;
                     const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
                     Pack<T, V> val[4];
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const T* src = entry_row<T>(a, code[u]);
-                        val[u] = src ? ld_entry<T, V, CG>(a, code[u], src + c) : zero_pack<T, V>();
+                        val[u] = src ? ld_src<T, V, CG>(src + c) : zero_pack<T, V>();
                     }
 #pragma unroll
                     for (int u = 0; u < 4; ++u) add_into(part, val[u]);
@@ -1910,8 +1850,6 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
     la.lim_state = a->num_nodes;
     la.lim_x = a->direction == GRG_B200_UP ? (a->by_individual ? a->num_individuals : a->num_samples) : a->num_mutations;
     la.lim_miss = a->num_mutations;
-    la.list_hint = (a->launch_flags & GRG_B200_LAUNCH_LISTS_EVICT_FIRST) != 0;
-    la.input_hint = a->direction == GRG_B200_DOWN && (a->launch_flags & GRG_B200_LAUNCH_INPUTS_EVICT_FIRST) != 0;
     if (a->dtype == GRG_B200_MIXED) {
         la.state_lo = static_cast<char*>(a->state) + GRG_B200_MIX_PLANE(a->num_nodes * a->ld_state * 4);
         if (a->direction == GRG_B200_DOWN) {  // levels read the encoded copies in mix_scratch

@@ -241,12 +241,6 @@ typedef struct grg_b200_traverse_args {
  * level lists until the hardware reports that kernel complete, and so overlaps the launch
  * gap.  Ignored when any level is streamed. */
 #define GRG_B200_LAUNCH_PDL 1
-/* L2 eviction priority hints (per load instruction; no cache or device setting changes): the
- * level lists (row pointers, row ids, heavy-row lists and gather codes), which a traversal
- * reads once, are loaded with L2 evict_first so they leave first and node rows stay cached. */
-#define GRG_B200_LAUNCH_LISTS_EVICT_FIRST 2
-/* The same hint on down input and miss rows (mutation rows, each read once per traversal). */
-#define GRG_B200_LAUNCH_INPUTS_EVICT_FIRST 4
 
 /*
  * GRG_B200_SCHEDULE_LEVELS: one launch per level (each level waits for the previous one).
