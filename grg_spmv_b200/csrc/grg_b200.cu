@@ -611,11 +611,8 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
 }
 
 // MB = CTAs per SM the register budget is sized for: 6 (narrow_variant 6, 40 registers), 5
-// (narrow_variant 7, 48 registers: no spills, fewer warps) or kQ2Blocks<V> (narrow_variant 8,
-// Q = 2: two quads, eight row fetches, in flight per round; a one-column lane holds a fetch in
-// two registers, so it keeps 5 CTAs per SM, wider lanes 3).
-template <int V>
-constexpr int kQ2Blocks = V == 1 ? 5 : 3;
+// (narrow_variant 7, 48 registers: no spills, fewer warps) or 3 (narrow_variant 8, Q = 2: two
+// quads, eight row fetches, in flight per round).
 template <typename T, int V, int INIT, int MB, int Q = 1>
 __global__ void __launch_bounds__(kNarrowThreads, MB) level_vec_kernel(LevelArgs a) {
     pdl_trigger();
@@ -1933,7 +1930,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
 #define GRG_FUSED(INIT)                                                                                  \
     if (variant == 8) {                                                                                  \
         if (la.log2s > 0) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, true, 6>, la, heavy_blocks)); \
-        else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, false, kQ2Blocks<V>, 2>, la, heavy_blocks)); \
+        else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_fused_kernel<T, V, INIT, false, 3, 2>, la, heavy_blocks));          \
     } else if (variant == 7 || variant == 9 || variant == 10) {                                          \
         GRG_FUSED_MB(INIT, 5)                                                                            \
     } else {                                                                                             \
@@ -1970,7 +1967,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         const int64_t warps = (narrow + (32 >> lg) - 1) >> (5 - lg);
         const dim3 grid(static_cast<unsigned>((warps + kNarrowWarps - 1) / kNarrowWarps));
 #define GRG_VEC(INIT)                                                                      \
-    if (variant == 8) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, kQ2Blocks<V>, 2>, la)); \
+    if (variant == 8) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 3, 2>, la)); \
     else if (variant == 7 || variant == 9 || variant == 10) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 5>, la)); \
     else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_vec_kernel<T, V, INIT, 6>, la));
         switch (init_mode) {

@@ -47,8 +47,7 @@ def test_header_constants_match_binding():
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
-@pytest.mark.parametrize("struct,cname", [(nat.Level, "grg_b200_level"), (nat.TraverseArgs, "grg_b200_traverse_args"),
-                                          (nat.RowopArgs, "grg_b200_rowop_args")])
+@pytest.mark.parametrize("struct,cname", [(nat.Level, "grg_b200_level"), (nat.TraverseArgs, "grg_b200_traverse_args")])
 def test_struct_layout_matches_c(tmp_path, struct, cname):
     fields = [f[0] for f in struct._fields_]
     src = tmp_path / "layout.c"
@@ -78,33 +77,6 @@ def test_invalid_arguments_fail_before_any_launch():
     args.narrow_variant = 11
     assert lib.grg_b200_traverse(ctypes.byref(args), None) == nat.ERR_INVALID
     assert "narrow_variant" in nat.last_error(lib)
-
-
-def test_rowop_rejects_bad_arguments_before_any_launch():
-    lib = nat.load_library()
-    args = nat.RowopArgs(rows=10, k=0, ld=4, src=16, dst=16)
-    assert lib.grg_b200_rowop(ctypes.byref(args), None) == nat.ERR_INVALID
-    assert "k >= 1" in nat.last_error(lib)
-    args = nat.RowopArgs(rows=10, k=4, ld=4, src=16, dst=16, col_sums=1)
-    assert lib.grg_b200_rowop(ctypes.byref(args), None) == nat.ERR_INVALID
-    assert "partials" in nat.last_error(lib)
-    args = nat.RowopArgs(rows=10, k=4, ld=4, src=16, dst=16, miss_in=16)
-    assert lib.grg_b200_rowop(ctypes.byref(args), None) == nat.ERR_INVALID
-    assert "miss_scale" in nat.last_error(lib)
-
-
-@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
-def test_rowop_block_count_matches_c(tmp_path):
-    rows = [0, 1, 255, 256, 257, 300_000, 10_000_000]
-    src = tmp_path / "blocks.c"
-    lines = ["#include <stdio.h>", '#include "grg_b200.h"', "int main(void) {"]
-    lines += [f'  printf("%lld\\n", (long long)GRG_B200_ROWOP_BLOCKS((long long){r}));' for r in rows]
-    lines += ["  return 0;", "}"]
-    src.write_text("\n".join(lines))
-    exe = tmp_path / "blocks"
-    subprocess.run(["gcc", f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
-    out = [int(x) for x in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
-    assert out == [nat.rowop_blocks(r) for r in rows]
 
 
 def test_ring_create_rejects_bad_sizes():
