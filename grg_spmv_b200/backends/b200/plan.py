@@ -86,6 +86,10 @@ class B200Plan:
     lists, plain precision; other calls fall back to "levels").
     ``persist_ctas``: with ``narrow_variant`` 9 or 10, the CTAs of a level launch's persistent
     narrow part (each walks row groups); 0 sizes it to what the GPU holds at once.
+    ``heavy_buckets``: with ``balance``, also group the heavy rows (the suffix) into
+    power-of-two length buckets.  Off by default: heavy rows then stay in row order (locality
+    order for down), so rows that share source rows run together.  On config 2 at k = 8 this
+    is what lets down level 0 read each parent row from DRAM about once.
     ``fuse_entries``: > 0 runs each stretch of consecutive resident levels with at most this many
     gather entries (default mode, plain precision, padded variants) as one cooperative launch
     with a grid barrier between levels instead of one launch per level; results are
@@ -107,6 +111,7 @@ class B200Plan:
     schedule: str = "levels"
     persist_ctas: int = 0
     fuse_entries: int = 0
+    heavy_buckets: bool = False
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:

@@ -298,14 +298,16 @@ class B200Runtime:
         if up_on:
             plan = lay.pair.plan_up
             built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance,
-                                                            plan.pad_lists, plan.long_first, plan.slots, device=list_device)}
+                                                            plan.pad_lists, plan.long_first, plan.slots, device=list_device,
+                                                            heavy_buckets=plan.heavy_buckets)}
             levels[Direction.UP] = self._upload_levels(art.levels_up, built)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
             plan = lay.pair.plan_down
             built = {lv.level: lv for lv in build_down_levels(
                 off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
-                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first, plan.slots, device=list_device)}
+                plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first, plan.slots, device=list_device,
+                heavy_buckets=plan.heavy_buckets)}
             levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
         del coo
         return _DeviceArtifact(

@@ -134,7 +134,7 @@ def _quad_class(counts: np.ndarray) -> np.ndarray:
 
 def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
             group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True,
-            pad: bool = False, long_first: bool = True, slots: bool = False) -> LevelGather:
+            pad: bool = False, long_first: bool = True, slots: bool = False, heavy_buckets: bool = False) -> LevelGather:
     """Stable-sort the concatenated pieces by row, flag segment starts, build row_ptr.
 
     With ``locality`` the rows are stored in the order of the id of their last state entry
@@ -170,15 +170,19 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
             key[rs[last]] = ids[state_pos[last]]
         perm = _stable_argsort(key)
     use_slots = slots and pad and balance
-    if balance and num_rows > 1:
-        if use_slots:  # buckets of equal padded width (power-of-two quads)
-            bucket = _quad_class(counts[perm])
-        else:
-            bucket = _bit_length(counts[perm])
-        perm = perm[_stable_argsort(-bucket if long_first else bucket)]
     heavy_mask = counts[perm] > heavy_threshold
-    perm = np.concatenate((perm[~heavy_mask], perm[heavy_mask]))
-    num_heavy = int(heavy_mask.sum())
+    narrow_perm, heavy_perm = perm[~heavy_mask], perm[heavy_mask]
+    if balance and narrow_perm.size > 1:
+        if use_slots:  # buckets of equal padded width (power-of-two quads)
+            bucket = _quad_class(counts[narrow_perm])
+        else:
+            bucket = _bit_length(counts[narrow_perm])
+        narrow_perm = narrow_perm[_stable_argsort(-bucket if long_first else bucket)]
+    if balance and heavy_buckets and heavy_perm.size > 1:
+        bucket = _bit_length(counts[heavy_perm])
+        heavy_perm = heavy_perm[_stable_argsort(-bucket if long_first else bucket)]
+    perm = np.concatenate((narrow_perm, heavy_perm))
+    num_heavy = int(heavy_perm.size)
     row_ids = None
     if not np.array_equal(perm, np.arange(num_rows)):
         lengths = counts[perm]
@@ -219,7 +223,8 @@ def _finish(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np
 
 def _finish_torch(level: int, row_begin: int, num_rows: int, rows: np.ndarray, ids: np.ndarray, src: np.ndarray,
                   group: np.ndarray, heavy_threshold: int, locality: bool = False, balance: bool = True,
-                  pad: bool = False, long_first: bool = True, slots: bool = False, device="cuda") -> LevelGather:
+                  pad: bool = False, long_first: bool = True, slots: bool = False, heavy_buckets: bool = False,
+                  device="cuda") -> LevelGather:
     """``_finish`` with PyTorch on ``device`` (the GPU when the runtime builds its levels):
     the same steps as the NumPy version, in integer arithmetic only, so the lists, row
     pointers, processing order and slot tables are identical to it."""
@@ -267,13 +272,17 @@ def _finish_torch(level: int, row_begin: int, num_rows: int, rows: np.ndarray, i
             width = torch.where(width < quads, width * 2, width)
         return torch.where(quads == 0, torch.zeros_like(width), width)
 
-    if balance and n > 1:
-        c = counts[perm]
-        bucket = quad_class(c) if use_slots else torch.searchsorted(pow2, c, right=True)
-        perm = perm[torch.sort(-bucket if long_first else bucket, stable=True).indices]
     heavy_mask = counts[perm] > int(heavy_threshold)
-    perm = torch.cat((perm[~heavy_mask], perm[heavy_mask]))
-    num_heavy = int(heavy_mask.sum())
+    narrow_perm, heavy_perm = perm[~heavy_mask], perm[heavy_mask]
+    if balance and narrow_perm.numel() > 1:
+        c = counts[narrow_perm]
+        bucket = quad_class(c) if use_slots else torch.searchsorted(pow2, c, right=True)
+        narrow_perm = narrow_perm[torch.sort(-bucket if long_first else bucket, stable=True).indices]
+    if balance and heavy_buckets and heavy_perm.numel() > 1:
+        bucket = torch.searchsorted(pow2, counts[heavy_perm], right=True)
+        heavy_perm = heavy_perm[torch.sort(-bucket if long_first else bucket, stable=True).indices]
+    perm = torch.cat((narrow_perm, heavy_perm))
+    num_heavy = int(heavy_perm.numel())
     row_ids = None
     if not torch.equal(perm, torch.arange(n, dtype=i64, device=dev)):
         lengths = counts[perm]
@@ -330,7 +339,7 @@ def load_blocks(blocks) -> dict[tuple[int, int], tuple[np.ndarray, np.ndarray]]:
 
 def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, locality: bool = False,
                     balance: bool = True, pad: bool = False, long_first: bool = True, slots: bool = False,
-                    device=None) -> list[LevelGather]:
+                    device=None, heavy_buckets: bool = False) -> list[LevelGather]:
     """Gather lists for up levels 1..h-1 (level 0 is seeded from the input); built with
     PyTorch on ``device`` when given (identical results), else with NumPy."""
     finish = _finish if device is None else (lambda *a: _finish_torch(*a, device=device))
@@ -349,7 +358,7 @@ def build_up_levels(level_offsets: np.ndarray, coo: dict, heavy_threshold: int, 
             src.append(np.full(r.size, s, dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         r, i, g = cat(rows, np.int64), cat(ids, np.int64), cat(src, np.int16)
-        levels.append(finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first, slots))
+        levels.append(finish(dst, int(off[dst]), n, r, i, np.zeros(i.size, np.uint8), g, heavy_threshold, locality, balance, pad, long_first, slots, heavy_buckets))
     return levels
 
 
@@ -364,7 +373,8 @@ def _selector_by_node(ptr: np.ndarray, idx: np.ndarray, num_rows: int) -> tuple[
 
 def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, heavy_threshold: int,
                       locality: bool = True, balance: bool = True, pad: bool = False,
-                      long_first: bool = True, slots: bool = False, device=None) -> list[LevelGather]:
+                      long_first: bool = True, slots: bool = False, device=None,
+                      heavy_buckets: bool = False) -> list[LevelGather]:
     """Gather lists for down levels h-1..0 in execution order (PyTorch on ``device`` when
     given, identical results).
 
@@ -400,7 +410,8 @@ def build_down_levels(level_offsets: np.ndarray, coo: dict, sel_mut, sel_miss, h
             grp.append(np.full(p.size, 2 + (h - 1 - s), dtype=np.int16))
         cat = (lambda parts, dt: np.concatenate(parts) if parts else np.empty(0, dtype=dt))
         levels.append(finish(dst, lo, hi - lo, cat(rows, np.int64), cat(ids, np.int64), cat(src, np.uint8),
-                              cat(grp, np.int16), heavy_threshold, locality, balance, pad, long_first, slots))
+                              cat(grp, np.int16), heavy_threshold, locality, balance, pad, long_first, slots,
+                              heavy_buckets))
     return levels
 
 

@@ -29,9 +29,12 @@ def _same(a, b):
 
 
 @pytest.mark.parametrize("opts", [dict(heavy=2, pad=True, slots=False, long_first=True),
+                                  dict(heavy=2, pad=True, slots=False, long_first=True, heavy_buckets=True),
                                   dict(heavy=128, pad=True, slots=True, long_first=True),
                                   dict(heavy=3, pad=False, slots=False, long_first=False),
-                                  dict(heavy=6, pad=True, slots=True, long_first=False)], ids=["pad", "slots", "plain", "slots-short"])
+                                  dict(heavy=3, pad=False, slots=False, long_first=False, heavy_buckets=True),
+                                  dict(heavy=6, pad=True, slots=True, long_first=False)],
+                         ids=["pad", "pad-heavy-buckets", "slots", "plain", "plain-heavy-buckets", "slots-short"])
 @pytest.mark.parametrize("name", NAMES)
 def test_torch_builder_matches_numpy(name, opts):
     from grg_spmv_b200.artifact import iter_artifact_blocks, load_grg_spmv_header
@@ -39,7 +42,7 @@ def test_torch_builder_matches_numpy(name, opts):
 
     st = load_grg_spmv_header(artifact_path(name), np.float64)
     coo = load_blocks(iter_artifact_blocks(artifact_path(name)))
-    kw = dict(pad=opts["pad"], long_first=opts["long_first"], slots=opts["slots"])
+    kw = dict(pad=opts["pad"], long_first=opts["long_first"], slots=opts["slots"], heavy_buckets=opts.get("heavy_buckets", False))
     for locality in (False, True):
         a = build_up_levels(st.level_offsets, coo, opts["heavy"], locality, True, **kw)
         b = build_up_levels(st.level_offsets, coo, opts["heavy"], locality, True, device="cpu", **kw)
@@ -92,3 +95,20 @@ def test_gpu_builder_matches_numpy():
         for x, y in zip(build_down_levels(st.level_offsets, coo, sel, miss, 2, True, True, True, slots=True),
                         build_down_levels(st.level_offsets, coo, sel, miss, 2, True, True, True, slots=True, device="cuda")):
             _same(x, y)
+
+
+def test_heavy_rows_keep_row_order_unless_bucketed():
+    """Heavy rows (the suffix) stay in row order by default and are grouped by length only with
+    ``heavy_buckets``; narrow rows are grouped by length either way."""
+    from grg_spmv_b200.backends.b200.structures import _finish
+
+    # row r has lengths[r] entries; threshold 4: rows 1, 3, 4 are heavy
+    lengths = np.asarray([2, 9, 1, 5, 20, 3])
+    rows = np.repeat(np.arange(lengths.size), lengths)
+    ids = np.arange(rows.size)
+    z = np.zeros(rows.size, dtype=np.int64)
+    plain = _finish(0, 0, lengths.size, rows, ids, z, z, 4)
+    assert list(plain.row_ids[-3:]) == [1, 3, 4]
+    assert list(plain.row_ids[:3]) == [0, 5, 2]  # narrow: 2 and 3 entries (bucket 2) in row order, then 1 entry
+    grouped = _finish(0, 0, lengths.size, rows, ids, z, z, 4, heavy_buckets=True)
+    assert list(grouped.row_ids[-3:]) == [4, 1, 3]  # 20 entries (bucket 5), then 9 and 5 (bucket 4) in row order
