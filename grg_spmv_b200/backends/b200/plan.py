@@ -83,7 +83,9 @@ class B200Plan:
     per level; default mode with ``narrow_variant`` 6 or 7 only).
     ``schedule``: "levels" (one launch per level) or "dataflow" (one persistent launch per
     traversal, rows wait only for their own sources; default mode, resident levels, padded
-    lists, plain precision; other calls fall back to "levels").
+    lists, plain precision; other calls fall back to "levels").  Its readiness sentinel is one
+    specific quiet NaN: an input holding exactly that NaN makes the wait time out (status
+    ``GRG_B200_DEVICE_WAIT_TIMEOUT``, undefined result).
     ``persist_ctas``: with ``narrow_variant`` 9 or 10, the CTAs of a level launch's persistent
     narrow part (each walks row groups); 0 sizes it to what the GPU holds at once.
     ``heavy_buckets``: with ``balance``, also group the heavy rows (the suffix) into
