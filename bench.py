@@ -85,8 +85,6 @@ def parse_args():
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
     p.add_argument("--heavy-buckets", action="store_true", help="also group heavy rows by length (default: row order)")
-    p.add_argument("--prefetch-lists", choices=["auto", "on", "off"], default="auto",
-                   help="L2 prefetch of each row's gather codes (default: the plan's)")
     p.add_argument("--slots", choices=["none", "up", "down", "both"], default="none",
                    help="directions whose narrow rows are padded to their bucket width (list offset from position)")
     p.add_argument("--pdl", choices=["auto", "on", "off"], default="auto",
@@ -314,8 +312,6 @@ def run_b200(args) -> None:
         extra["long_first"] = False
     if args.heavy_buckets:
         extra["heavy_buckets"] = True
-    if args.prefetch_lists != "auto":
-        extra["prefetch_lists"] = args.prefetch_lists == "on"
     if args.pdl != "auto":
         extra["pdl"] = args.pdl == "on"
     if args.narrow_split is not None:
@@ -675,8 +671,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "heavy_buckets": pair.plan_down.heavy_buckets,
-                       "prefetch_lists": pair.plan_down.prefetch_lists, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
+                       "long_first": pair.plan_down.long_first, "heavy_buckets": pair.plan_down.heavy_buckets, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",

@@ -92,8 +92,6 @@ class B200Plan:
     power-of-two length buckets.  Off by default: heavy rows then stay in row order (locality
     order for down), so rows that share source rows run together.  On config 2 at k = 8 this
     is what lets down level 0 read each parent row from DRAM about once.
-    ``prefetch_lists``: the level kernels prefetch each row's gather codes into L2 as soon as
-    the row's extent is known (``GRG_B200_LAUNCH_PREFETCH_LISTS``).
     ``fuse_entries``: > 0 runs each stretch of consecutive resident levels with at most this many
     gather entries (default mode, plain precision, padded variants) as one cooperative launch
     with a grid barrier between levels instead of one launch per level; results are
@@ -116,7 +114,6 @@ class B200Plan:
     persist_ctas: int = 0
     fuse_entries: int = 0
     heavy_buckets: bool = False
-    prefetch_lists: bool = False
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:

@@ -215,19 +215,7 @@ struct LevelArgs {
     void* state_lo;
     const void* x_lo;
     const void* miss_lo;
-    int32_t prefetch_lists;  // GRG_B200_LAUNCH_PREFETCH_LISTS
 };
-
-// Prefetch the gather codes [e0, e1) of a row into L2, one 32-byte sector (8 codes) per lane
-// of the `lanes` lanes that share the row, starting with lane `lane`.  Only addresses inside the
-// row's list are named; the prefetch holds no registers and completes asynchronously.
-__device__ __forceinline__ void prefetch_codes(const LevelArgs& a, int32_t e0, int32_t e1, int lane, int lanes) {
-    if (!a.prefetch_lists) return;
-    for (int32_t sct = (e0 >> 3) + lane; (sct << 3) < e1; sct += lanes) {
-        const uint32_t* p = a.entries + (sct << 3 > e0 ? sct << 3 : e0);
-        asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
-    }
-}
 
 enum DeviceError : int32_t {
     kErrStateId = 1,
@@ -507,7 +495,6 @@ __device__ __forceinline__ void vec_rows(const LevelArgs& a, int64_t block) {
     int32_t e0, e1;
     narrow_extent(a, pos, e0, e1);
     const int glane = lane & ((1 << a.log2g) - 1);
-    prefetch_codes(a, e0, e1, glane, 1 << a.log2g);
     const int64_t row = level_row(a, pos);
     const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
     const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
@@ -588,7 +575,6 @@ __device__ __forceinline__ void split_rows(const LevelArgs& a, int64_t block) {
         e0 = __ldg(a.row_ptr + pos);
         e1 = __ldg(a.row_ptr + pos + 1);
         row = level_row(a, pos);
-        prefetch_codes(a, e0, e1, lane & ((1 << lg) - 1), 1 << lg);
     }
     pdl_wait();
     const int glane = lane & ((1 << a.log2g) - 1);
@@ -649,7 +635,6 @@ __device__ __forceinline__ void warp_heavy_rows(const LevelArgs& a, int64_t bloc
     const int64_t pos = __ldg(a.heavy_rows + w);
     const int32_t e0 = __ldg(a.row_ptr + pos);
     const int32_t e1 = __ldg(a.row_ptr + pos + 1);
-    prefetch_codes(a, e0, e1, lane32, 32);
     const int64_t row = level_row(a, pos);
     pdl_wait();
     const int g_lanes = 1 << a.log2g;
@@ -1865,7 +1850,6 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
     la.lim_state = a->num_nodes;
     la.lim_x = a->direction == GRG_B200_UP ? (a->by_individual ? a->num_individuals : a->num_samples) : a->num_mutations;
     la.lim_miss = a->num_mutations;
-    la.prefetch_lists = (a->launch_flags & GRG_B200_LAUNCH_PREFETCH_LISTS) != 0;
     if (a->dtype == GRG_B200_MIXED) {
         la.state_lo = static_cast<char*>(a->state) + GRG_B200_MIX_PLANE(a->num_nodes * a->ld_state * 4);
         if (a->direction == GRG_B200_DOWN) {  // levels read the encoded copies in mix_scratch

@@ -241,10 +241,6 @@ typedef struct grg_b200_traverse_args {
  * level lists until the hardware reports that kernel complete, and so overlaps the launch
  * gap.  Ignored when any level is streamed. */
 #define GRG_B200_LAUNCH_PDL 1
-/* Level kernels prefetch each row's gather codes into L2 (prefetch.global.L2, one 32-byte
- * sector per lane) as soon as the row's extent is known, so that the code loads of later
- * rounds wait on L2 rather than DRAM. */
-#define GRG_B200_LAUNCH_PREFETCH_LISTS 2
 
 /*
  * GRG_B200_SCHEDULE_LEVELS: one launch per level (each level waits for the previous one).
