@@ -18,8 +18,10 @@ ops' shared ``io0`` buffer).  Metric: edge·RHS/s = steps · 2·E·k / device ti
   around each direction's level launches, issued back to back as in the recorded graph (a
   second pass with events around every launch prints the per-level breakdown to stderr).  Algorithmic bytes per level: 4 per gather entry and row
   pointer, plus each destination row written once and read once later (2·k·8); plus, for
-  down, the mutation and miss input rows read once.  ``traffic`` is the DRAM traffic of the
-  level kernels per step from the committed ncu summary (medium graph, scaled by edges).
+  down, the mutation and miss input rows read once.  ``traffic`` is the DRAM traffic (read +
+  write) of one up-level-1 launch measured by ncu on the same configuration;
+  ``traffic_launches`` lists it with down levels 3 and 0, beside this run's own timing and
+  algorithmic bytes of those launches.
 * ``cpu_baseline``: the oracle (SciPy restatement of the reference's ReferenceRuntime) on one
   step of the same graph, RHS columns split over one process per host core (up to k), rank 0,
   N=1 only.
@@ -221,21 +223,15 @@ def measured_peak_hbm() -> tuple[float, str]:
     return 6650.0, "fallback"
 
 
-def profiled_traffic(num_edges: int, k: int, precision: str, schedule: str):
-    """DRAM bytes per step of the level kernels, from the ncu summary committed under
-    profiles/ (measured on the medium graph at k = 8, FP64, per-level schedule, L2 kept warm)
-    and scaled by edges; None for other configurations."""
-    path = REPO / "profiles" / "level_traffic_medium_k8.md"
-    if k != 8 or precision != "plain" or schedule != "levels" or not path.exists():
-        return None, None
-    text = path.read_text()
-    import re
-
-    t = re.search(r"traffic_per_step_bytes_medium: (\d+)", text)
-    e = re.search(r"edges_medium: (\d+)", text)
-    if not t or not e:
-        return None, None
-    return int(t.group(1)) * num_edges / int(e.group(1)), f"{path.relative_to(REPO)} (medium graph, scaled by edges)"
+# DRAM bytes (read + write) and ncu duration of single level launches on the config-2 graph at
+# k = 8, FP64, default plan, measured with ncu -c 1 and L2 left warm (profiles/
+# level_traffic_config2_k8.md gives the commands).  Keys: (direction, level).
+CONFIG2_K8_TRAFFIC = {
+    ("up", 1): {"kernel": "level_fused_kernel", "dram_bytes": 12047360 + 256, "ncu_us": 29.12},
+    ("down", 3): {"kernel": "level_fused_kernel", "dram_bytes": 127070720 + 21648640, "ncu_us": 39.04},
+    ("down", 0): {"kernel": "level_warp_kernel", "dram_bytes": 457896448 + 17945088, "ncu_us": 242.94},
+}
+TRAFFIC_SOURCE = "profiles/level_traffic_config2_k8.md (ncu -c 1 per launch on the config-2 graph, k = 8)"
 
 
 def traversal_level_launches(levels, fused_heavy: bool, fuse_entries: int) -> int:
@@ -506,10 +502,14 @@ def run_b200(args) -> None:
             print(f"[traversal] {name} entries={sum(u[1] for u in units)} ms={level_ms[name]:.4f}", file=sys.stderr)
             lv_bytes += level_bytes(units, k, vb, name, M, use_miss=True)
         per_level_ms = 0.0
+        launch_ms = {}  # (direction, level) -> ms of that level's launch, events around it alone
         for name, _, _, units in all_evs:
-            for (_, a, b, lv), unit in zip([x for x in per_level if x[0] == name], units):
+            lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
+            lv_ids = [L for L in lv_order if scan.level_sizes[L] > 0]
+            for (_, a, b, lv), unit, L in zip([x for x in per_level if x[0] == name], units, lv_ids):
                 ms = a.elapsed_time(b)
                 per_level_ms += ms
+                launch_ms[(name, L)] = (ms, level_bytes([unit], k, vb, "up", M, False))
                 nbytes = level_bytes([unit], k, vb, "up", M, False)
                 print(f"[level] {name} rows={unit[0]} entries={unit[1]} heavy={lv.num_heavy} "
                       f"ms={ms:.4f} GB/s={nbytes / ms / 1e6:.1f}", file=sys.stderr)
@@ -650,7 +650,21 @@ def run_b200(args) -> None:
             tiers["multi_graph"], tiers["multi_graph_small_blocks"] = measure_tiers(
                 args, multi, device, stream, [config_blocks, [1, 1, 2, 3, 3, 4]])
             tiers["multi_graph"]["generate_s"] = gen_multi
-    traffic, traffic_src = profiled_traffic(E, k, args.precision, pair.plan_down.schedule)
+    # Per-launch view of the captured launches: this run's own event timing of each launch (events
+    # around it alone) and its algorithmic bytes, beside the DRAM bytes ncu measured for the same
+    # launch of the same configuration.
+    traffic, traffic_launches = None, None
+    captured = (args.workload == "config2" and k == 8 and args.precision == "plain" and pair.plan_down.schedule == "levels"
+                and not args.heavy_buckets and launch_ms)
+    if captured:
+        traffic_launches = []
+        for (direction, level), cap in CONFIG2_K8_TRAFFIC.items():
+            ms, alg = launch_ms.get((direction, level), (None, None))
+            traffic_launches.append({"launch": f"{direction} level {level}", "kernel": cap["kernel"], "dram_bytes": cap["dram_bytes"],
+                                     "algorithmic_bytes": alg, "traffic_over_algorithmic": cap["dram_bytes"] / alg if alg else None,
+                                     "ms_this_run": ms, "achieved_gbs_this_run": alg / ms / 1e6 if ms else None,
+                                     "ncu_us": cap["ncu_us"]})
+        traffic = CONFIG2_K8_TRAFFIC[("up", 1)]["dram_bytes"]
     if rank == 0:
         line = {
             "metric": METRIC,
@@ -680,8 +694,9 @@ def run_b200(args) -> None:
                        "vram_budget_frac": args.budget_frac, "streamed_bytes_per_step": int(streamed_bytes),
                        "ring_slots": layout.allocated_ring_buffer_size},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "traffic_unit": "bytes per up+down step (level kernels)",
-                         "traffic_source": traffic_src, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
+                         "traffic": traffic, "traffic_unit": "DRAM bytes of one launch: up level 1 (level_fused_kernel)",
+                         "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
+                         "traffic_launches": traffic_launches, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
                                     if pair.plan_down.schedule == "dataflow" else
                                     "level gathers (one fused narrow+heavy launch per level)"),
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
