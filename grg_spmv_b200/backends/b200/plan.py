@@ -120,10 +120,10 @@ class B200Plan:
             raise ValueError(f"heavy_threshold must be >= 1, got {self.heavy_threshold}")
         if self.row_order not in (None, "natural", "locality"):
             raise ValueError(f"row_order must be 'natural' or 'locality', got {self.row_order!r}")
-        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < 11:
-            raise ValueError(f"narrow_variant must be in [0, 11), got {self.narrow_variant}")
+        if self.narrow_variant is not None and not 0 <= int(self.narrow_variant) < nat.NARROW_VARIANTS:
+            raise ValueError(f"narrow_variant must be in [0, {nat.NARROW_VARIANTS}), got {self.narrow_variant}")
         if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
-            raise ValueError("narrow_variants 6-10 read padded gather lists; they need pad_lists=True")
+            raise ValueError(f"narrow_variants 6-{nat.NARROW_VARIANTS - 1} read padded gather lists; they need pad_lists=True")
         if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3):
             raise ValueError(f"heavy_variant must be 0, 1, 2 or 3, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:

@@ -215,6 +215,7 @@ struct LevelArgs {
     void* state_lo;
     const void* x_lo;
     const void* miss_lo;
+    int32_t up;  // an up level: its lists name state rows (and null padding) only
 };
 
 enum DeviceError : int32_t {
@@ -717,6 +718,153 @@ __global__ void __launch_bounds__(kNarrowThreads, MB) level_fused_kernel(LevelAr
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) warp_heavy_rows<T, V, INIT>(a, blockIdx.x);
     else if constexpr (SPLIT) split_rows<T, V, INIT>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
     else vec_rows<T, V, INIT, Q>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+}
+
+// Lean row walks (narrow_variant 11 and 12): the same rows and the same arithmetic as
+// vec_rows / warp_heavy_rows, for the common launch: no bounds checks (the launch has no error
+// word), source rows addressed with one 32 x 32 -> 64-bit multiply (row ids and leading
+// dimensions are below 2^32), and for up levels a state-only decode (up lists name state rows
+// and null padding only; input rows reach up through the level-0 seed).  SEG = true keeps a
+// fresh partial sum per segment, so results are bit-identical to vec_rows; SEG = false adds a
+// row's entries left to right into one sum (default mode only: integer-valued inputs stay
+// exact, real-valued ones differ from the reference by reassociation).
+template <typename T, bool UPONLY>
+__device__ __forceinline__ const T* lean_source(const LevelArgs& a, uint32_t code, bool& ok) {
+    const uint32_t id = code & GRG_B200_ID_MASK;
+    const uint32_t src = (code >> GRG_B200_SRC_SHIFT) & GRG_B200_SRC_MASK;
+    if constexpr (UPONLY) {
+        ok = src == GRG_B200_SRC_STATE;
+        return static_cast<const T*>(a.state) + static_cast<size_t>(id) * static_cast<uint32_t>(a.ld_state);
+    } else {
+        ok = src == GRG_B200_SRC_STATE || src == GRG_B200_SRC_INPUT || (src == GRG_B200_SRC_MISS && a.use_miss);
+        const T* base = src == GRG_B200_SRC_STATE ? static_cast<const T*>(a.state)
+                                                   : (src == GRG_B200_SRC_INPUT ? static_cast<const T*>(a.x) : static_cast<const T*>(a.miss));
+        const uint32_t ld = static_cast<uint32_t>(src == GRG_B200_SRC_STATE ? a.ld_state : (src == GRG_B200_SRC_INPUT ? a.ld_x : a.ld_miss));
+        return base + static_cast<size_t>(id) * ld;
+    }
+}
+
+template <typename T, int V, int INIT, bool SEG, bool UPONLY>
+__device__ __forceinline__ void lean_rows(const LevelArgs& a, int64_t block) {
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    if (pos >= narrow) return;  // no warp-wide operations below
+    const int32_t q0 = __ldg(a.row_ptr + pos) >> 2;
+    const int32_t q1 = __ldg(a.row_ptr + pos + 1) >> 2;
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int64_t row = level_row(a, pos);
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    const uint4 first = q0 < q1 ? __ldg(codes4 + q0) : null4;  // static list: before the wait
+    pdl_wait();
+    T* state = static_cast<T*>(a.state);
+    const int step = V << a.log2g;
+    const int k = static_cast<int>(a.k);
+    for (int c = glane * V; c < k; c += step) {
+        Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+        Pack<T, V> seg = zero_pack<T, V>();
+        uint4 cur = first;
+        for (int32_t q = q0; q < q1; ++q) {
+            const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+            const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+            Pack<T, V> val[4];
+            bool ok[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const T* p = lean_source<T, UPONLY>(a, code[u], ok[u]);
+                val[u] = ok[u] ? ld_ro<T, V>(p + c) : zero_pack<T, V>();
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if constexpr (SEG) {
+                    if (code[u] & GRG_B200_SEG_START) {
+                        add_into(acc, seg);
+                        seg = zero_pack<T, V>();
+                    }
+                    if (ok[u]) add_into(seg, val[u]);
+                } else {
+                    if (ok[u]) add_into(acc, val[u]);
+                }
+            }
+            cur = nxt;
+        }
+        if constexpr (SEG) add_into(acc, seg);
+        st_pack(state + row * a.ld_state + c, acc);
+    }
+}
+
+// Heavy rows, one warp each, as warp_heavy_rows (padded lists) with the lean decode.
+template <typename T, int V, int INIT, bool UPONLY, int WPC = kWarpRowThreads / 32>
+__device__ __forceinline__ void lean_heavy_rows(const LevelArgs& a, int64_t block) {
+    const int64_t w = block * WPC + (threadIdx.x >> 5);
+    if (w >= a.num_heavy) return;  // warp-uniform
+    const int lane32 = threadIdx.x & 31;
+    const int64_t pos = __ldg(a.heavy_rows + w);
+    const int32_t q1 = __ldg(a.row_ptr + pos + 1) >> 2;
+    const int32_t qs = __ldg(a.row_ptr + pos) >> 2;
+    const int64_t row = level_row(a, pos);
+    pdl_wait();
+    const int g_lanes = 1 << a.log2g;
+    const int groups = 32 >> a.log2g;
+    const int glane = lane32 & (g_lanes - 1);
+    const int grp = lane32 >> a.log2g;
+    T* state = static_cast<T*>(a.state);
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    const int step = V << a.log2g;
+    const int k = static_cast<int>(a.k);
+    for (int base = 0; base < k; base += step) {  // uniform trip count across the warp
+        const int c = base + glane * V;
+        const bool active = c < k;
+        Pack<T, V> part = zero_pack<T, V>();
+        if (active) {
+            int32_t q = qs + grp;
+            uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
+            for (; q < q1; q += groups) {
+                const uint4 nxt = q + groups < q1 ? __ldg(codes4 + q + groups) : null4;
+                const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+                Pack<T, V> val[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    bool ok;
+                    const T* p = lean_source<T, UPONLY>(a, code[u], ok);
+                    val[u] = ok ? ld_ro<T, V>(p + c) : zero_pack<T, V>();
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) add_into(part, val[u]);
+                cur = nxt;
+            }
+        }
+        for (int off = 16; off >= g_lanes; off >>= 1) {
+            const Pack<T, V> other = shfl_xor_pack(part, off);
+            add_into(part, other);
+        }
+        if (grp == 0 && active) {
+            Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
+            add_into(acc, part);
+            st_pack(state + row * a.ld_state + c, acc);
+        }
+    }
+}
+
+// narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
+// level_fused_kernel; MB = 5 CTAs per SM.
+template <typename T, int V, int INIT, bool SEG, bool UPONLY>
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_lean_kernel(LevelArgs a, int64_t heavy_blocks) {
+    pdl_trigger();
+    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, V, INIT, UPONLY>(a, blockIdx.x);
+    else lean_rows<T, V, INIT, SEG, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+}
+
+// All-heavy levels under narrow_variant 11 / 12: the lean heavy walk alone.
+template <typename T, int V, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kWarpRowThreads) level_lean_warp_kernel(LevelArgs a) {
+    pdl_trigger();
+    lean_heavy_rows<T, V, INIT, UPONLY>(a, blockIdx.x);
 }
 
 // Narrow rows of padded lists, persistent (narrow_variant 9 and 10).  The narrow CTAs of a
@@ -1850,6 +1998,7 @@ LevelArgs level_args(const grg_b200_traverse_args* a, const Shape& sh) {
     la.lim_state = a->num_nodes;
     la.lim_x = a->direction == GRG_B200_UP ? (a->by_individual ? a->num_individuals : a->num_samples) : a->num_mutations;
     la.lim_miss = a->num_mutations;
+    la.up = a->direction == GRG_B200_UP;
     if (a->dtype == GRG_B200_MIXED) {
         la.state_lo = static_cast<char*>(a->state) + GRG_B200_MIX_PLANE(a->num_nodes * a->ld_state * 4);
         if (a->direction == GRG_B200_DOWN) {  // levels read the encoded copies in mix_scratch
@@ -1911,6 +2060,43 @@ template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, int persist_ctas, bool pdl,
                        cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
+    // the lean walks (11, 12) serve launches without an error word and without row splits;
+    // others fall back to variant 7's kernels
+    const bool lean = (variant == 11 || variant == 12) && la.err == nullptr && !exact && heavy_variant == 2 &&
+                      la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
+    if (variant == 11 || variant == 12) {
+        if (lean && narrow > 0 && la.log2s == 0) {
+            constexpr int rows_per_cta = kWarpRowThreads / 32;
+            const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
+            const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+            const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
+#define GRG_LEAN(INIT)                                                                                                                if (variant == 11) {                                                                                                                  if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_lean_kernel<T, V, INIT, true, true>, la, heavy_blocks));          else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_lean_kernel<T, V, INIT, true, false>, la, heavy_blocks));            } else {                                                                                                                              if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_lean_kernel<T, V, INIT, false, true>, la, heavy_blocks));         else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_lean_kernel<T, V, INIT, false, false>, la, heavy_blocks));           }
+            switch (init_mode) {
+                case 0: GRG_LEAN(0) break;
+                case 1: GRG_LEAN(1) break;
+                case 2: GRG_LEAN(2) break;
+                default: GRG_LEAN(3) break;
+            }
+#undef GRG_LEAN
+            GRG_LAUNCH_CHECK("level_lean_kernel");
+            return GRG_B200_OK;
+        }
+        if (lean && narrow == 0 && la.num_heavy > 0) {
+            constexpr int rows_per_cta = kWarpRowThreads / 32;
+            const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
+#define GRG_LEAN_WARP(INIT)                                                                                                            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_kernel<T, V, INIT, true>, la));                    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_kernel<T, V, INIT, false>, la));
+            switch (init_mode) {
+                case 0: GRG_LEAN_WARP(0) break;
+                case 1: GRG_LEAN_WARP(1) break;
+                case 2: GRG_LEAN_WARP(2) break;
+                default: GRG_LEAN_WARP(3) break;
+            }
+#undef GRG_LEAN_WARP
+            GRG_LAUNCH_CHECK("level_lean_warp_kernel");
+            return GRG_B200_OK;
+        }
+        variant = 7;
+    }
     const bool padded_variant = variant >= 6 && variant <= 10;
     const bool persist = (variant == 9 || variant == 10) && la.log2s == 0 && la.num_rows < (int64_t{1} << 30);
     // fused launch, except for all-heavy levels (e.g. down level 0, where every sample row is
@@ -2077,7 +2263,7 @@ int launch_level_mx_typed(const LevelArgs& la, int init_mode, cudaStream_t s) {
 
 // Mixed level launches: narrow_variant 7 walks rows with 2 columns per lane, others with 4.
 int launch_level_mx(LevelArgs la, int init_mode, int variant, cudaStream_t s) {
-    const int vm = variant == 7 ? 2 : 4;
+    const int vm = variant == 7 || variant == 11 || variant == 12 ? 2 : 4;
     const int64_t cols = (la.k + vm - 1) / vm;
     int log2g = 0;
     while ((1 << log2g) < cols && log2g < 5) ++log2g;
@@ -2172,7 +2358,7 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
 // warp each, no row split).  `la` receives the level's launch parameters.
 bool run_eligible(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level& L, LevelArgs& la) {
     if (a->fuse_entries <= 0 || a->exact_order || a->dtype == GRG_B200_MIXED || a->heavy_variant != 2) return false;
-    if (a->narrow_variant < 6 || a->narrow_variant == 8 || !a->dataflow_sync) return false;
+    if (a->narrow_variant < 6 || a->narrow_variant == 8 || a->narrow_variant == 12 || !a->dataflow_sync) return false;
     if (L.ring_slot >= 0 || L.num_rows <= 0 || L.num_entries > a->fuse_entries || L.list_align != 4) return false;
     if (L.num_heavy < 0 || L.num_heavy > L.num_rows || L.num_rows >= (int64_t{1} << 30)) return false;
     if (build_level_args(a, sh, &L, L.blob, la) != GRG_B200_OK) return false;

@@ -205,7 +205,16 @@ typedef struct grg_b200_traverse_args {
                                            persistent: the narrow CTAs are capped at the resident
                                            count and each warp walks row groups, loading the next
                                            group's row pointers and first codes while the current
-                                           rows load; 10: as 9 with 64 registers (4 CTAs per SM). */
+                                           rows load; 10: as 9 with 64 registers (4 CTAs per SM);
+                                           11: as 7 with a lean walk for launches without an
+                                           error word (no bounds checks, 32 x 32-bit row
+                                           addressing, state-only decode on up levels, heavy rows
+                                           likewise), bit-identical to 7; 12: as 11 but a row's
+                                           entries are summed left to right into one partial sum
+                                           (no per-segment restarts; default mode only).
+                                           11 and 12 fall back to 7 with an error word, split
+                                           rows or exact order.  Up level lists name state rows
+                                           and null padding only. */
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
@@ -254,7 +263,7 @@ typedef struct grg_b200_traverse_args {
 typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
 #define GRG_B200_DEVICE_WAIT_TIMEOUT 6
 
-#define GRG_B200_NARROW_VARIANTS 11
+#define GRG_B200_NARROW_VARIANTS 13
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

@@ -53,7 +53,7 @@ def _cases_by_artifact():
 GROUPS = _cases_by_artifact()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12])
 @pytest.mark.parametrize("heavy", [128, 2], ids=["narrow", "heavy-rows"])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
@@ -128,3 +128,30 @@ def test_golden_mixed_precision(group, heavy, golden_data):
             if case["miss"] and case["direction"] == "up" and integer:
                 np.testing.assert_array_equal(miss, golden_data[case["key"] + "|miss_out"], err_msg=case["key"])
         assert runtime.device_error() == 0
+
+
+@pytest.mark.parametrize("variant", [11, 12])
+@pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
+def test_golden_lean_walks(group, variant, golden_data):
+    """The lean walks on every golden case (no bounds-check word, rows not split, no heavy
+    rows): variant 11 keeps the per-segment partial sums and reproduces the reference bit for
+    bit; variant 12 sums each row in one partial sum, exact for integer-valued inputs and within
+    tolerance otherwise."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
+
+    name, dtype = group
+    plan = B200Plan(narrow_variant=variant, heavy_variant=2, heavy_threshold=128, narrow_split=0)
+    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), pair=B200PlanPair(plan_up=plan, plan_down=plan))
+    rtol, atol = (RTOL_F64, ATOL_F64) if dtype == "float64" else (RTOL_F32, ATOL_F32)
+    with B200Runtime(layout, check_bounds=False) as runtime:
+        (grg,) = runtime.grgs
+        for case in GROUPS[group]:
+            out, miss = _run_case(grg, case, golden_data)
+            expected = golden_data[case["key"] + "|out"]
+            integer = any(tag in case["case"] for tag in ("pm1", "ones", "zeros"))
+            if variant == 11 or (integer and case["init"] is None):
+                np.testing.assert_array_equal(out, expected, err_msg=case["key"])
+            else:
+                np.testing.assert_allclose(out, expected, rtol=rtol, atol=atol * max(1.0, np.abs(expected).max()), err_msg=case["key"])
+            if case["miss"] and case["direction"] == "up" and variant == 11:
+                np.testing.assert_array_equal(miss, golden_data[case["key"] + "|miss_out"], err_msg=case["key"])

@@ -612,3 +612,48 @@ def test_fused_level_runs_are_bit_identical(synth_artifact, k, fuse):
     x_up, x_dn, miss, _ = inputs
     np.testing.assert_allclose(results[entries][0], oracle.matmul(x_up, "up"), rtol=1e-12, atol=1e-9)
     np.testing.assert_allclose(results[entries][3], oracle.matmul(x_dn, "down", miss=miss.copy()), rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("k", [1, 3, 8, 16, 33])
+def test_lean_walks_match_variant_7_and_the_oracle(synth_artifact, k):
+    """Narrow variants 11 and 12 (the lean walks, used by launches without a bounds-check word
+    and without row splits) on every mode of the hot path: 11 returns the same bits as 7; 12
+    (one partial sum per row) is exact for integer-valued inputs and within 1e-12 otherwise."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
+
+    oracle = OracleGRG(synth_artifact)
+    results = {}
+    for variant in (7, 11, 12):
+        plan = B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=2, narrow_split=0)
+        layout = _layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=B200PlanPair(plan_up=plan, plan_down=plan))
+        rng = np.random.default_rng(300 + k)  # the same inputs for every variant
+        with B200Runtime(layout, check_bounds=False) as runtime:
+            (grg,) = runtime.grgs
+            S, M, N, I = grg.num_samples, grg.num_mutations, grg.num_nodes, grg.num_individuals
+            out = []
+            for direction, cols in (("up", S), ("down", M)):
+                xi, xr = _pm1(rng, (k, cols)), rng.standard_normal((k, cols))
+                out.append(("int", grg.matmul(xi, direction), oracle.matmul(xi, direction)))
+                out.append(("real", grg.matmul(xr, direction), oracle.matmul(xr, direction)))
+                init = rng.standard_normal(k)
+                out.append(("real", grg.matmul(xr, direction, init=init), oracle.matmul(xr, direction, init=init)))
+                out.append(("real", grg.matmul(xr, direction, init="xtx"), oracle.matmul(xr, direction, init="xtx")))
+                mat = rng.standard_normal((k, N))
+                out.append(("real", grg.matmul(xr, direction, init=mat, emit_all_nodes=True),
+                            oracle.matmul(xr, direction, init=mat, emit_all_nodes=True)))
+            xi = _pm1(rng, (k, I))
+            miss_b, miss_o = np.zeros((k, M)), np.zeros((k, M))
+            out.append(("int", grg.matmul(xi, "up", by_individual=True, miss=miss_b),
+                        oracle.matmul(xi, "up", by_individual=True, miss=miss_o)))
+            out.append(("int", miss_b, miss_o))
+            xd, miss = _pm1(rng, (k, M)), _pm1(rng, (k, M))
+            out.append(("int", grg.matmul(xd, "down", by_individual=True, miss=miss.copy()),
+                        oracle.matmul(xd, "down", by_individual=True, miss=miss.copy())))
+            results[variant] = out
+    for (kind, got7, ref), (_, got11, _), (_, got12, _) in zip(results[7], results[11], results[12]):
+        np.testing.assert_array_equal(got11, got7)
+        if kind == "int":
+            np.testing.assert_array_equal(got12, ref)
+            np.testing.assert_array_equal(got7, ref)
+        else:
+            np.testing.assert_allclose(got12, ref, rtol=1e-12, atol=1e-9)
