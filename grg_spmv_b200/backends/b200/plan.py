@@ -31,6 +31,7 @@ import warnings
 import numpy as np
 
 from grg_spmv_b200.artifact import ArtifactScan, scan_grg_spmv
+from grg_spmv_b200.backends.b200 import _native as nat
 from grg_spmv_b200.backends.b200.structures import blob_layout, down_entry_bound, up_entry_bound
 from grg_spmv_b200.types import Direction
 
