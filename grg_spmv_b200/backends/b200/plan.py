@@ -62,8 +62,9 @@ class B200Plan:
     ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
     processed together); None picks the direction's default (up natural, down locality).
     ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``); None
-    picks per call from the padded-list kernels (7 for k <= 16, 6 above, as measured on
-    B200; with ``pad_lists=False``, 5).
+    picks per call, as measured on B200: the lean walk 12 for k >= 2 in the default mode (7 at
+    k = 1); in exact order 7 for k <= 16 and 6 above; with ``pad_lists=False``, 5.  Runtimes
+    with bounds checking run 7 in place of 11 and 12.
     ``balance``: group narrow rows by length (power-of-two buckets) so a warp's rows finish
     together.
     ``autotune``: time the narrow-kernel variants, then the heavy-row kernels, when the runtime
@@ -142,7 +143,11 @@ class B200Plan:
             return int(self.narrow_variant)
         if not self.pad_lists:
             return 5
-        return 7 if int(k) <= 16 else 6
+        if self.exact_order:
+            return 7 if int(k) <= 16 else 6
+        # the lean walk with one partial sum per row: measured on B200 (config 2) +17% over 7 at
+        # k = 8 and +14% over 6 at k = 32; at k = 1 all three are within 1%
+        return 12 if int(k) >= 2 else 7
 
     def resolve_pdl(self, k: int) -> bool:
         """Whether calls with ``k`` right-hand sides use programmatic dependent launch."""
