@@ -227,9 +227,9 @@ def measured_peak_hbm() -> tuple[float, str]:
 # k = 8, FP64, default plan, measured with ncu -c 1 and L2 left warm (profiles/
 # level_traffic_config2_k8.md gives the commands).  Keys: (direction, level).
 CONFIG2_K8_TRAFFIC = {
-    ("up", 1): {"kernel": "level_fused_kernel", "dram_bytes": 12047360 + 256, "ncu_us": 29.12},
-    ("down", 3): {"kernel": "level_fused_kernel", "dram_bytes": 127070720 + 21648640, "ncu_us": 39.04},
-    ("down", 0): {"kernel": "level_warp_kernel", "dram_bytes": 457896448 + 17945088, "ncu_us": 242.94},
+    ("up", 1): {"kernel": "level_lean_kernel", "dram_bytes": 12035584 + 256, "ncu_us": 23.36},
+    ("down", 3): {"kernel": "level_lean_kernel", "dram_bytes": 126864896 + 21399040, "ncu_us": 34.53},
+    ("down", 0): {"kernel": "level_lean_warp_kernel", "dram_bytes": 459662592 + 19444480, "ncu_us": 211.33},
 }
 TRAFFIC_SOURCE = "profiles/level_traffic_config2_k8.md (ncu -c 1 per launch on the config-2 graph, k = 8)"
 
@@ -655,7 +655,7 @@ def run_b200(args) -> None:
     # launch of the same configuration.
     traffic, traffic_launches = None, None
     captured = (args.workload == "config2" and k == 8 and args.precision == "plain" and pair.plan_down.schedule == "levels"
-                and not args.heavy_buckets and launch_ms)
+                and not args.heavy_buckets and narrow_used == {"up": 12, "down": 12} and launch_ms)
     if captured:
         traffic_launches = []
         for (direction, level), cap in CONFIG2_K8_TRAFFIC.items():
@@ -694,7 +694,7 @@ def run_b200(args) -> None:
                        "vram_budget_frac": args.budget_frac, "streamed_bytes_per_step": int(streamed_bytes),
                        "ring_slots": layout.allocated_ring_buffer_size},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "traffic_unit": "DRAM bytes of one launch: up level 1 (level_fused_kernel)",
+                         "traffic": traffic, "traffic_unit": "DRAM bytes of one launch: up level 1 (level_lean_kernel)",
                          "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
                          "traffic_launches": traffic_launches, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
                                     if pair.plan_down.schedule == "dataflow" else

@@ -851,6 +851,91 @@ __device__ __forceinline__ void lean_heavy_rows(const LevelArgs& a, int64_t bloc
     }
 }
 
+// 32-byte vector loads and stores (sm_100): one chunk of 4 doubles or 8 floats.
+template <typename T>
+struct Chunk32 {
+    static constexpr int C = 32 / static_cast<int>(sizeof(T));
+    using type = Pack<T, C>;
+};
+
+template <typename T>
+__device__ __forceinline__ typename Chunk32<T>::type ld_chunk(const T* p) {
+    typename Chunk32<T>::type r;
+    if constexpr (std::is_same<T, double>::value) {
+        asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+                     : "=d"(r.v[0]), "=d"(r.v[1]), "=d"(r.v[2]), "=d"(r.v[3]) : "l"(p));
+    } else {
+        asm volatile("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                     : "=f"(r.v[0]), "=f"(r.v[1]), "=f"(r.v[2]), "=f"(r.v[3]), "=f"(r.v[4]), "=f"(r.v[5]), "=f"(r.v[6]), "=f"(r.v[7])
+                     : "l"(p));
+    }
+    return r;
+}
+
+// Narrow rows, entry-parallel (narrow_variant 13, default mode only).  A row's lane group of G
+// lanes is W chunk lanes x 2 entry slots (W = k / C, C columns per 32-byte chunk): lane (e, w)
+// adds chunk w of entries e and e + 2 of every 4-entry quad, so each code is decoded by W lanes
+// instead of G and a row fetch is one 32-byte load per chunk.  The two slots' sums are added by
+// one shuffle and the slot-0 lanes store.  The order of additions differs from the reference's
+// (exact for integer-valued inputs, reassociation otherwise).  log2w = log2(W), G = 2W.
+template <typename T, int INIT, bool UPONLY>
+__device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
+    using Ch = typename Chunk32<T>::type;
+    constexpr int C = Chunk32<T>::C;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    const bool live = pos < narrow;  // dead lanes still join the shuffle
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int log2w = a.log2g - 1;
+    const int w = glane & ((1 << log2w) - 1);
+    const int e = glane >> log2w;  // entry slot 0 or 1
+    int32_t q0 = 0, q1 = 0;
+    int64_t row = 0;
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    uint4 cur = null4;
+    if (live) {
+        q0 = __ldg(a.row_ptr + pos) >> 2;
+        q1 = __ldg(a.row_ptr + pos + 1) >> 2;
+        row = level_row(a, pos);
+        if (q0 < q1) cur = __ldg(codes4 + q0);  // static list: before the wait
+    }
+    pdl_wait();
+    const int c = w * C;
+    Ch acc = zero_pack<T, C>();
+    for (int32_t q = q0; q < q1; ++q) {
+        const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+        const uint32_t c0 = e == 0 ? cur.x : cur.y;  // entries e and e + 2 of the quad
+        const uint32_t c1 = e == 0 ? cur.z : cur.w;
+        bool ok0, ok1;
+        const T* p0 = lean_source<T, UPONLY>(a, c0, ok0);
+        const T* p1 = lean_source<T, UPONLY>(a, c1, ok1);
+        const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
+        const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+        add_into(acc, v0);
+        add_into(acc, v1);
+        cur = nxt;
+    }
+    const Ch other = shfl_xor_pack(acc, 1 << log2w);
+    if (live && e == 0) {
+        Ch out = init_value<T, C, INIT>(a, row, c);
+        add_into(out, acc);
+        add_into(out, other);
+        st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
+    }
+}
+
+// narrow_variant 13: heavy rows (lean walk) first, then the entry-parallel narrow rows.
+template <typename T, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks) {
+    pdl_trigger();
+    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, blockIdx.x);
+    else entry_rows<T, INIT, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+}
+
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
 // level_fused_kernel; MB = 5 CTAs per SM.
 template <typename T, int V, int INIT, bool SEG, bool UPONLY>
