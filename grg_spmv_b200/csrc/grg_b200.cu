@@ -2147,8 +2147,26 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     // the lean walks (11, 12) serve launches without an error word and without row splits;
     // others fall back to variant 7's kernels
-    const bool lean = (variant == 11 || variant == 12) && la.err == nullptr && !exact && heavy_variant == 2 &&
+    const bool lean = (variant == 11 || variant == 12 || variant == 13) && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
+    if (variant == 13) {  // entry-parallel narrow rows where the shape allows it, else as 12
+        constexpr int C = Chunk32<T>::C;
+        const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
+                           (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
+                           (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
+                           (!la.use_miss || aligned(la.miss, 32));
+        if (shape) {
+            constexpr int rows_per_cta = kWarpRowThreads / 32;
+            const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
+            const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+            const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
+            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks));
+            else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks));
+            GRG_LAUNCH_CHECK("level_entry_kernel");
+            return GRG_B200_OK;
+        }
+        variant = 12;
+    }
     if (variant == 11 || variant == 12) {
         if (lean && narrow > 0 && la.log2s == 0) {
             constexpr int rows_per_cta = kWarpRowThreads / 32;
@@ -2348,7 +2366,7 @@ int launch_level_mx_typed(const LevelArgs& la, int init_mode, cudaStream_t s) {
 
 // Mixed level launches: narrow_variant 7 walks rows with 2 columns per lane, others with 4.
 int launch_level_mx(LevelArgs la, int init_mode, int variant, cudaStream_t s) {
-    const int vm = variant == 7 || variant == 11 || variant == 12 ? 2 : 4;
+    const int vm = variant == 7 || variant >= 11 ? 2 : 4;
     const int64_t cols = (la.k + vm - 1) / vm;
     int log2g = 0;
     while ((1 << log2g) < cols && log2g < 5) ++log2g;
@@ -2443,7 +2461,7 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
 // warp each, no row split).  `la` receives the level's launch parameters.
 bool run_eligible(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level& L, LevelArgs& la) {
     if (a->fuse_entries <= 0 || a->exact_order || a->dtype == GRG_B200_MIXED || a->heavy_variant != 2) return false;
-    if (a->narrow_variant < 6 || a->narrow_variant == 8 || a->narrow_variant == 12 || !a->dataflow_sync) return false;
+    if (a->narrow_variant < 6 || a->narrow_variant == 8 || a->narrow_variant >= 12 || !a->dataflow_sync) return false;
     if (L.ring_slot >= 0 || L.num_rows <= 0 || L.num_entries > a->fuse_entries || L.list_align != 4) return false;
     if (L.num_heavy < 0 || L.num_heavy > L.num_rows || L.num_rows >= (int64_t{1} << 30)) return false;
     if (build_level_args(a, sh, &L, L.blob, la) != GRG_B200_OK) return false;

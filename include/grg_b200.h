@@ -211,10 +211,14 @@ typedef struct grg_b200_traverse_args {
                                            addressing, state-only decode on up levels, heavy rows
                                            likewise), bit-identical to 7; 12: as 11 but a row's
                                            entries are summed left to right into one partial sum
-                                           (no per-segment restarts; default mode only).
-                                           11 and 12 fall back to 7 with an error word, split
-                                           rows or exact order.  Up level lists name state rows
-                                           and null padding only. */
+                                           (no per-segment restarts; default mode only);
+                                           13: as 12 with entry-parallel narrow rows: a row's
+                                           lanes form two entry slots, each lane adding one
+                                           32-byte chunk of every other entry (k = 2^n x the
+                                           vector width, no init, 32-byte aligned buffers;
+                                           otherwise as 12).  11 to 13 fall back to 7 with an
+                                           error word, split rows or exact order.  Up level
+                                           lists name state rows and null padding only. */
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
                                            (list staged in shared memory, tree reduction); 1 one
                                            warp per row (lane groups split the list, shuffle
@@ -263,7 +267,7 @@ typedef struct grg_b200_traverse_args {
 typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
 #define GRG_B200_DEVICE_WAIT_TIMEOUT 6
 
-#define GRG_B200_NARROW_VARIANTS 13
+#define GRG_B200_NARROW_VARIANTS 14
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

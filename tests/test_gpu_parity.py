@@ -53,7 +53,7 @@ def _cases_by_artifact():
 GROUPS = _cases_by_artifact()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13])
 @pytest.mark.parametrize("heavy", [128, 2], ids=["narrow", "heavy-rows"])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
@@ -130,13 +130,13 @@ def test_golden_mixed_precision(group, heavy, golden_data):
         assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("variant", [11, 12])
+@pytest.mark.parametrize("variant", [11, 12, 13])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_lean_walks(group, variant, golden_data):
     """The lean walks on every golden case (no bounds-check word, rows not split, no heavy
     rows): variant 11 keeps the per-segment partial sums and reproduces the reference bit for
-    bit; variant 12 sums each row in one partial sum, exact for integer-valued inputs and within
-    tolerance otherwise."""
+    bit; variants 12 and 13 sum each row in one or two partial sums, exact for integer-valued
+    inputs and within tolerance otherwise."""
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
 
     name, dtype = group
