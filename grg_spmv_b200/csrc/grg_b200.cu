@@ -928,10 +928,9 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
     }
 }
 
-// narrow_variant 13 (MB = 5 CTAs per SM) and 14 (MB = 6, 40 registers): heavy rows (lean walk)
-// first, then the entry-parallel narrow rows.
-template <typename T, int INIT, bool UPONLY, int MB>
-__global__ void __launch_bounds__(kNarrowThreads, MB) level_entry_kernel(LevelArgs a, int64_t heavy_blocks) {
+// narrow_variant 13: heavy rows (lean walk) first, then the entry-parallel narrow rows.
+template <typename T, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks) {
     pdl_trigger();
     if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, blockIdx.x);
     else entry_rows<T, INIT, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
@@ -2148,9 +2147,9 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     // the lean walks (11, 12) serve launches without an error word and without row splits;
     // others fall back to variant 7's kernels
-    const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
+    const bool lean = (variant == 11 || variant == 12 || variant == 13) && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
-    if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
+    if (variant == 13) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
         const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
                            (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
@@ -2161,13 +2160,8 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
             const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
             const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
-            if (variant == 13) {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true, 5>, la, heavy_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false, 5>, la, heavy_blocks));
-            } else {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true, 6>, la, heavy_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false, 6>, la, heavy_blocks));
-            }
+            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks));
+            else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks));
             GRG_LAUNCH_CHECK("level_entry_kernel");
             return GRG_B200_OK;
         }
