@@ -73,7 +73,7 @@ def test_bench_cpu_helpers(monkeypatch):
     import bench
 
     args = bench.parse_args()
-    assert args.k == 8 and args.e2e_inflight == 4 and args.pdl == "auto" and args.slots == "none"
+    assert args.k == 8 and args.e2e_inflight == 8 and args.pdl == "auto" and args.slots == "none"
     spec = bench.large_spec(0.1)
     assert (spec.num_samples, spec.num_nodes, spec.num_mutations, spec.num_levels) == (100_000, 6_000_000, 2_000_000, 60)
 
