@@ -193,6 +193,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def workload_description(name: str, scan, streamed: bool) -> str:
+    """The workload string both arms report: the configuration's name and the graph's sizes."""
+    return (f"{name}: S={scan.num_samples}, levels={scan.num_levels}, N={scan.num_nodes}, E={scan.num_edges}, "
+            f"M={scan.num_mutations}, 1% missing, {'levels partly streamed' if streamed else 'fully resident'}, up+down per step")
+
+
 def host_info(workers: int) -> dict:
     """What every CPU number is recorded with: the host's logical CPUs and physical cores, its
     CPU model, and the processes x threads the measurement actually used."""
@@ -680,8 +686,7 @@ def run_b200(args) -> None:
             "vs_baseline": None,
             "dtype": "f64" if args.precision == "plain" else "f64 sums, f32+i16 node state",
             "data": "synthetic (seeded generator with the configuration's shapes; no public GRG dataset offline)",
-            "config": {"workload": f"{args.workload}: S={S}, levels={scan.num_levels}, N={grg.num_nodes}, E={E}, M={M}, "
-                                   f"1% missing, {'fully resident' if not streamed_bytes else 'levels partly streamed'}, up+down per step",
+            "config": {"workload": workload_description(args.workload, scan, streamed=bool(streamed_bytes)),
                        "k": k, "precision": args.precision, "num_samples": S, "num_nodes": grg.num_nodes, "num_edges": E, "num_mutations": M,
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
@@ -952,6 +957,8 @@ def run_reference(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from grg_spmv_b200.artifact import scan_grg_spmv
+
     path, _ = make_artifact(args, 0)
     with np.load(path) as data:
         S, M, E = (int(np.asarray(data[key]).item()) for key in ("num_samples", "num_mutations", "num_edges"))
@@ -977,7 +984,8 @@ def run_reference(args) -> None:
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}", "k": k, "num_edges": E},
+        "config": {"workload": workload_description(args.workload, scan_grg_spmv(path), streamed=False), "k": k,
+                   "precision": "plain", "num_samples": S, "num_edges": E, "num_mutations": M},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": sample, **host_info(workers)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
