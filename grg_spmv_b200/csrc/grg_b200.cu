@@ -928,6 +928,94 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
     }
 }
 
+// As entry_rows, with the codes of the row's first kPreQuads quads loaded before the wait
+// (narrow_variant 14): a lane keeps its two codes of each (8 registers), so rows of up to
+// 4 * kPreQuads entries walk their rounds without a code load on the critical path, and the
+// loads overlap the previous level under programmatic dependent launch.  Longer rows load the
+// rest one round ahead, as entry_rows does.
+constexpr int kPreQuads = 4;
+
+template <typename T, int INIT, bool UPONLY>
+__device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block) {
+    using Ch = typename Chunk32<T>::type;
+    constexpr int C = Chunk32<T>::C;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    const bool live = pos < narrow;  // dead lanes still join the shuffle
+    const int glane = lane & ((1 << a.log2g) - 1);
+    const int log2w = a.log2g - 1;
+    const int w = glane & ((1 << log2w) - 1);
+    const int e = glane >> log2w;  // entry slot 0 or 1
+    int32_t q0 = 0, q1 = 0;
+    int64_t row = 0;
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    uint32_t pre0[kPreQuads], pre1[kPreQuads];  // this lane's entries e and e + 2 of the first quads
+#pragma unroll
+    for (int j = 0; j < kPreQuads; ++j) pre0[j] = pre1[j] = null_code;
+    if (live) {
+        q0 = __ldg(a.row_ptr + pos) >> 2;
+        q1 = __ldg(a.row_ptr + pos + 1) >> 2;
+        row = level_row(a, pos);
+#pragma unroll
+        for (int j = 0; j < kPreQuads; ++j) {
+            if (q0 + j < q1) {  // static list: before the wait
+                const uint4 cq = __ldg(codes4 + q0 + j);
+                pre0[j] = e == 0 ? cq.x : cq.y;
+                pre1[j] = e == 0 ? cq.z : cq.w;
+            }
+        }
+    }
+    pdl_wait();
+    const int c = w * C;
+    Ch acc = zero_pack<T, C>();
+#pragma unroll
+    for (int j = 0; j < kPreQuads; ++j) {
+        if (q0 + j < q1) {
+            bool ok0, ok1;
+            const T* p0 = lean_source<T, UPONLY>(a, pre0[j], ok0);
+            const T* p1 = lean_source<T, UPONLY>(a, pre1[j], ok1);
+            const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
+            const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+            add_into(acc, v0);
+            add_into(acc, v1);
+        }
+    }
+    if (q0 + kPreQuads < q1) {
+        const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+        uint4 cur = __ldg(codes4 + q0 + kPreQuads);
+        for (int32_t q = q0 + kPreQuads; q < q1; ++q) {
+            const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+            const uint32_t c0 = e == 0 ? cur.x : cur.y;
+            const uint32_t c1 = e == 0 ? cur.z : cur.w;
+            bool ok0, ok1;
+            const T* p0 = lean_source<T, UPONLY>(a, c0, ok0);
+            const T* p1 = lean_source<T, UPONLY>(a, c1, ok1);
+            const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
+            const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+            add_into(acc, v0);
+            add_into(acc, v1);
+            cur = nxt;
+        }
+    }
+    const Ch other = shfl_xor_pack(acc, 1 << log2w);
+    if (live && e == 0) {
+        Ch out = init_value<T, C, INIT>(a, row, c);
+        add_into(out, acc);
+        add_into(out, other);
+        st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
+    }
+}
+
+template <typename T, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks) {
+    pdl_trigger();
+    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, blockIdx.x);
+    else entry_rows_pre<T, INIT, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+}
+
 // narrow_variant 13: heavy rows (lean walk) first, then the entry-parallel narrow rows.
 template <typename T, int INIT, bool UPONLY>
 __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks) {
@@ -2147,9 +2235,9 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
     // the lean walks (11, 12) serve launches without an error word and without row splits;
     // others fall back to variant 7's kernels
-    const bool lean = (variant == 11 || variant == 12 || variant == 13) && la.err == nullptr && !exact && heavy_variant == 2 &&
+    const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
-    if (variant == 13) {  // entry-parallel narrow rows where the shape allows it, else as 12
+    if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
         const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
                            (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
@@ -2160,8 +2248,13 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
             const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
             const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
-            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks));
-            else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks));
+            if (variant == 13) {
+                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks));
+                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks));
+            } else {
+                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, true>, la, heavy_blocks));
+                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, false>, la, heavy_blocks));
+            }
             GRG_LAUNCH_CHECK("level_entry_kernel");
             return GRG_B200_OK;
         }
