@@ -662,7 +662,7 @@ def run_b200(args) -> None:
     # launch of the same configuration.
     traffic, traffic_launches = None, None
     captured = (args.workload == "config2" and k == 8 and args.precision == "plain" and pair.plan_down.schedule == "levels"
-                and not args.heavy_buckets and narrow_used == {"up": 13, "down": 13} and launch_ms)
+                and not args.heavy_buckets and narrow_used == {"up": 14, "down": 14} and launch_ms)
     if captured:
         traffic_launches = []
         for (direction, level), cap in CONFIG2_K8_TRAFFIC.items():
