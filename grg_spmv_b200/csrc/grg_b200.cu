@@ -1024,75 +1024,6 @@ __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArg
     else entry_rows<T, INIT, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
 }
 
-// Heavy rows as lean_heavy_rows, with two quads (eight row fetches) per lane group in flight
-// each round (narrow_variant 15 on levels whose rows are all heavy): lane group g takes quads
-// g and g + groups of every 2 * groups.  The order of additions differs from lean_heavy_rows
-// (default mode: exact for integer-valued inputs).
-template <typename T, int V, int INIT, bool UPONLY>
-__device__ __forceinline__ void lean_heavy_rows_q2(const LevelArgs& a, int64_t block) {
-    constexpr int WPC = kWarpRowThreads / 32;
-    const int64_t w = block * WPC + (threadIdx.x >> 5);
-    if (w >= a.num_heavy) return;  // warp-uniform
-    const int lane32 = threadIdx.x & 31;
-    const int64_t pos = __ldg(a.heavy_rows + w);
-    const int32_t q1 = __ldg(a.row_ptr + pos + 1) >> 2;
-    const int32_t qs = __ldg(a.row_ptr + pos) >> 2;
-    const int64_t row = level_row(a, pos);
-    const int g_lanes = 1 << a.log2g;
-    const int groups = 32 >> a.log2g;
-    const int glane = lane32 & (g_lanes - 1);
-    const int grp = lane32 >> a.log2g;
-    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
-    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
-    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
-    uint4 cur0 = qs + grp < q1 ? __ldg(codes4 + qs + grp) : null4;  // static list: before the wait
-    uint4 cur1 = qs + grp + groups < q1 ? __ldg(codes4 + qs + grp + groups) : null4;
-    pdl_wait();
-    T* state = static_cast<T*>(a.state);
-    const int step = V << a.log2g;
-    const int k = static_cast<int>(a.k);
-    for (int base = 0; base < k; base += step) {  // uniform trip count across the warp
-        const int c = base + glane * V;
-        const bool active = c < k;
-        Pack<T, V> part = zero_pack<T, V>();
-        if (active) {
-            uint4 a0 = cur0, a1 = cur1;
-            for (int32_t q = qs + grp; q < q1; q += 2 * groups) {
-                const int32_t n0 = q + 2 * groups, n1 = q + 3 * groups;
-                const uint4 b0 = n0 < q1 ? __ldg(codes4 + n0) : null4;
-                const uint4 b1 = n1 < q1 ? __ldg(codes4 + n1) : null4;
-                const uint32_t code[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-                Pack<T, V> val[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    bool ok;
-                    const T* p = lean_source<T, UPONLY>(a, code[u], ok);
-                    val[u] = ok ? ld_ro<T, V>(p + c) : zero_pack<T, V>();
-                }
-#pragma unroll
-                for (int u = 0; u < 8; ++u) add_into(part, val[u]);
-                a0 = b0;
-                a1 = b1;
-            }
-        }
-        for (int off = 16; off >= g_lanes; off >>= 1) {
-            const Pack<T, V> other = shfl_xor_pack(part, off);
-            add_into(part, other);
-        }
-        if (grp == 0 && active) {
-            Pack<T, V> acc = init_value<T, V, INIT>(a, row, c);
-            add_into(acc, part);
-            st_pack(state + row * a.ld_state + c, acc);
-        }
-    }
-}
-
-template <typename T, int V, int INIT, bool UPONLY>
-__global__ void __launch_bounds__(kWarpRowThreads, 4) level_lean_warp_q2_kernel(LevelArgs a) {
-    pdl_trigger();
-    lean_heavy_rows_q2<T, V, INIT, UPONLY>(a, blockIdx.x);
-}
-
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
 // level_fused_kernel; MB = 5 CTAs per SM.
 template <typename T, int V, int INIT, bool SEG, bool UPONLY>
@@ -2306,23 +2237,6 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
-    if (variant == 15 && lean && narrow == 0 && la.num_heavy > 0) {  // all-heavy level: two quads per group per round
-        constexpr int rows_per_cta = kWarpRowThreads / 32;
-        const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
-#define GRG_LEAN_Q2(INIT)                                                                                                          \
-    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_q2_kernel<T, V, INIT, true>, la));             \
-    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_q2_kernel<T, V, INIT, false>, la));
-        switch (init_mode) {
-            case 0: GRG_LEAN_Q2(0) break;
-            case 1: GRG_LEAN_Q2(1) break;
-            case 2: GRG_LEAN_Q2(2) break;
-            default: GRG_LEAN_Q2(3) break;
-        }
-#undef GRG_LEAN_Q2
-        GRG_LAUNCH_CHECK("level_lean_warp_q2_kernel");
-        return GRG_B200_OK;
-    }
-    if (variant == 15) variant = 14;
     if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
         const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&

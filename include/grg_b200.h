@@ -217,10 +217,8 @@ typedef struct grg_b200_traverse_args {
                                            32-byte chunk of every other entry (k = 2^n x the
                                            vector width, no init, 32-byte aligned buffers;
                                            otherwise as 12); 14: as 13 with the codes of a row's
-                                           first 4 quads loaded before the previous level ends;
-                                           15: as 14, and levels whose rows are all heavy run
-                                           two quads per lane group per round.
-                                           11 to 15 fall back to 7 with an
+                                           first 4 quads loaded before the previous level ends.
+                                           11 to 14 fall back to 7 with an
                                            error word, split rows or exact order.  Up level
                                            lists name state rows and null padding only. */
     int32_t heavy_variant;              /* heavy-row kernel outside exact order: 0 one CTA per row
@@ -271,7 +269,7 @@ typedef struct grg_b200_traverse_args {
 typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
 #define GRG_B200_DEVICE_WAIT_TIMEOUT 6
 
-#define GRG_B200_NARROW_VARIANTS 16
+#define GRG_B200_NARROW_VARIANTS 15
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);
