@@ -234,9 +234,9 @@ def measured_peak_hbm() -> tuple[float, str]:
 # k = 8, FP64, default plan, measured with ncu -c 1 and L2 left warm (profiles/
 # level_traffic_config2_k8.md gives the commands).  Keys: (direction, level).
 CONFIG2_K8_TRAFFIC = {
-    ("up", 1): {"kernel": "level_entry_kernel", "dram_bytes": 12041216 + 0, "ncu_us": 25.73},
-    ("down", 3): {"kernel": "level_entry_kernel", "dram_bytes": 126808576 + 21081088, "ncu_us": 34.50},
-    ("down", 0): {"kernel": "level_lean_warp_kernel", "dram_bytes": 458143232 + 17050368, "ncu_us": 208.32},
+    ("up", 1): {"kernel": "level_entry_pre_kernel", "dram_bytes": 12044288 + 117248, "ncu_us": 25.28},
+    ("down", 3): {"kernel": "level_entry_pre_kernel", "dram_bytes": 126673920 + 21044480, "ncu_us": 34.43},
+    ("down", 0): {"kernel": "level_lean_warp_kernel", "dram_bytes": 458017280 + 17091328, "ncu_us": 208.90},
 }
 TRAFFIC_SOURCE = "profiles/level_traffic_config2_k8.md (ncu -c 1 per launch on the config-2 graph, k = 8)"
 
@@ -700,7 +700,7 @@ def run_b200(args) -> None:
                        "vram_budget_frac": args.budget_frac, "streamed_bytes_per_step": int(streamed_bytes),
                        "ring_slots": layout.allocated_ring_buffer_size},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": traffic, "traffic_unit": "DRAM bytes of one launch: up level 1 (level_entry_kernel)",
+                         "traffic": traffic, "traffic_unit": "DRAM bytes of one launch: up level 1 (level_entry_pre_kernel)",
                          "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
                          "traffic_launches": traffic_launches, "kernel": ("dataflow traversal (sentinel fill + persistent gather kernel + seed/output), per direction"
                                     if pair.plan_down.schedule == "dataflow" else
