@@ -88,6 +88,8 @@ def parse_args():
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
     p.add_argument("--heavy-buckets", action="store_true", help="also group heavy rows by length (default: row order)")
+    p.add_argument("--no-short-rows", action="store_true",
+                   help="walk the one-quad narrow rows with two entry slots like the rest (default: one slot)")
     p.add_argument("--slots", choices=["none", "up", "down", "both"], default="none",
                    help="directions whose narrow rows are padded to their bucket width (list offset from position)")
     p.add_argument("--pdl", choices=["auto", "on", "off"], default="auto",
@@ -315,6 +317,8 @@ def run_b200(args) -> None:
         extra["long_first"] = False
     if args.heavy_buckets:
         extra["heavy_buckets"] = True
+    if args.no_short_rows:
+        extra["short_rows"] = False
     if args.pdl != "auto":
         extra["pdl"] = args.pdl == "on"
     if args.narrow_split is not None:
@@ -662,7 +666,7 @@ def run_b200(args) -> None:
     # launch of the same configuration.
     traffic, traffic_launches = None, None
     captured = (args.workload == "config2" and k == 8 and args.precision == "plain" and pair.plan_down.schedule == "levels"
-                and not args.heavy_buckets and narrow_used == {"up": 14, "down": 14} and launch_ms)
+                and not args.heavy_buckets and not args.no_short_rows and narrow_used == {"up": 14, "down": 14} and launch_ms)
     if captured:
         traffic_launches = []
         for (direction, level), cap in CONFIG2_K8_TRAFFIC.items():
@@ -691,7 +695,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "heavy_buckets": pair.plan_down.heavy_buckets, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
+                       "long_first": pair.plan_down.long_first, "heavy_buckets": pair.plan_down.heavy_buckets, "short_rows": pair.plan_down.short_rows, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",

@@ -17,7 +17,7 @@ REPO_DIR = PACKAGE_DIR.parent
 LIB_PATH = PACKAGE_DIR / "libgrg_b200.so"
 SOURCES = (PACKAGE_DIR / "csrc" / "grg_b200.cu",)
 HEADER_DIR = REPO_DIR / "include"
-ABI_VERSION = 13
+ABI_VERSION = 14
 
 NVCC_FLAGS = (
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -79,6 +79,7 @@ class Level(ctypes.Structure):
         ("slot_pos", ctypes.c_int64 * 8),
         ("slot_entry", ctypes.c_int64 * 8),
         ("slot_width", ctypes.c_int32 * 8),
+        ("short_rows", ctypes.c_int64),
     ]
 
 

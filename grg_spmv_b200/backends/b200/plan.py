@@ -95,6 +95,9 @@ class B200Plan:
     power-of-two length buckets.  Off by default: heavy rows then stay in row order (locality
     order for down), so rows that share source rows run together.  On config 2 at k = 8 this
     is what lets down level 0 read each parent row from DRAM about once.
+    ``short_rows``: let narrow variants 13 and 14 walk each level's narrow suffix of lists of at
+    most one quad (4 entries) with one entry slot, so a CTA covers twice the rows there.  On
+    by default; most rows of the upper down levels are that short.
     ``fuse_entries``: > 0 runs each stretch of consecutive resident levels with at most this many
     gather entries (default mode, plain precision, padded variants) as one cooperative launch
     with a grid barrier between levels instead of one launch per level; results are
@@ -117,6 +120,7 @@ class B200Plan:
     persist_ctas: int = 0
     fuse_entries: int = 0
     heavy_buckets: bool = False
+    short_rows: bool = True
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -171,7 +175,8 @@ class B200Plan:
     @classmethod
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
-                   "heavy_variant", "long_first", "narrow_split", "schedule", "slots", "pdl", "persist_ctas", "fuse_entries"}
+                   "heavy_variant", "long_first", "narrow_split", "schedule", "slots", "pdl", "persist_ctas", "fuse_entries",
+                   "heavy_buckets", "short_rows"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -183,7 +188,8 @@ class B200Plan:
                    long_first=bool(value.get("long_first", True)), narrow_split=int(value.get("narrow_split", -1)),
                    schedule=str(value.get("schedule", "levels")), slots=bool(value.get("slots", False)),
                    pdl=None if value.get("pdl") is None else bool(value.get("pdl")),
-                   persist_ctas=int(value.get("persist_ctas", 0)), fuse_entries=int(value.get("fuse_entries", 0)))
+                   persist_ctas=int(value.get("persist_ctas", 0)), fuse_entries=int(value.get("fuse_entries", 0)),
+                   heavy_buckets=bool(value.get("heavy_buckets", False)), short_rows=bool(value.get("short_rows", True)))
 
 
 @dataclass(frozen=True)

@@ -300,7 +300,7 @@ class B200Runtime:
             built = {lv.level: lv for lv in build_up_levels(off, coo, plan.heavy_threshold, plan.locality(Direction.UP), plan.balance,
                                                             plan.pad_lists, plan.long_first, plan.slots, device=list_device,
                                                             heavy_buckets=plan.heavy_buckets)}
-            levels[Direction.UP] = self._upload_levels(art.levels_up, built)
+            levels[Direction.UP] = self._upload_levels(art.levels_up, built, plan.short_rows)
         if down_on:
             sel_miss = (st.sel_miss.indptr, st.sel_miss.indices, st.num_mutations) if req.need_down_miss_input else None
             plan = lay.pair.plan_down
@@ -308,7 +308,7 @@ class B200Runtime:
                 off, coo, (st.sel_mut.indptr, st.sel_mut.indices, st.num_mutations), sel_miss, plan.heavy_threshold,
                 plan.locality(Direction.DOWN), plan.balance, plan.pad_lists, plan.long_first, plan.slots, device=list_device,
                 heavy_buckets=plan.heavy_buckets)}
-            levels[Direction.DOWN] = self._upload_levels(art.levels_down, built)
+            levels[Direction.DOWN] = self._upload_levels(art.levels_down, built, plan.short_rows)
         del coo
         return _DeviceArtifact(
             path=art.path,
@@ -328,7 +328,7 @@ class B200Runtime:
             level0_rows=int(off[1]) if off.size > 1 else 0,
         )
 
-    def _upload_levels(self, plans, built) -> _DeviceLevels:
+    def _upload_levels(self, plans, built, short_rows: bool = True) -> _DeviceLevels:
         import torch
 
         arr = (nat.Level * len(plans))()
@@ -349,7 +349,8 @@ class B200Runtime:
             arr[i] = nat.Level(row_begin=lv.row_begin, num_rows=lv.num_rows, num_entries=lv.num_entries,
                                num_heavy=int(lv.heavy_rows.size), heavy_threshold=lv.heavy_threshold, ring_slot=slot,
                                blob=blob.data_ptr(), blob_bytes=nbytes, off_row_ptr=off_ptr, off_heavy=off_heavy,
-                               off_row_ids=off_ids, off_entries=off_entries, list_align=lv.list_align)
+                               off_row_ids=off_ids, off_entries=off_entries, list_align=lv.list_align,
+                               short_rows=lv.short_rows() if short_rows else 0)
             if lv.slots is not None:
                 arr[i].num_slot_buckets = int(lv.slots.shape[0])
                 for b, (pos, entry, width) in enumerate(lv.slots):

@@ -82,6 +82,17 @@ class LevelGather:
     def num_entries(self) -> int:
         return int(self.entries.size)
 
+    def short_rows(self) -> int:
+        """The longest suffix of the narrow positions whose lists hold at most one quad (4
+        entries): the rows the entry-parallel walks take with one entry slot.  Under the
+        default long-first bucketing these are all narrow rows of at most 3 entries (and the
+        empty ones).  0 for unpadded lists."""
+        narrow = self.num_rows - int(self.heavy_rows.size)
+        if self.list_align != 4 or narrow <= 0:
+            return 0
+        longer = np.flatnonzero(np.diff(self.row_ptr[:narrow + 1].astype(np.int64)) > 4)
+        return narrow - (int(longer[-1]) + 1 if longer.size else 0)
+
     def layout(self) -> tuple[int, int, int, int, int]:
         return blob_layout(self.num_rows, self.heavy_rows.size, self.entries.size, self.row_ids is not None)
 

@@ -216,6 +216,7 @@ struct LevelArgs {
     const void* x_lo;
     const void* miss_lo;
     int32_t up;  // an up level: its lists name state rows (and null padding) only
+    int64_t short_rows;  // entry kernels: the last short_rows narrow positions take one entry slot
 };
 
 enum DeviceError : int32_t {
@@ -884,7 +885,7 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
     constexpr int C = Chunk32<T>::C;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t narrow = a.num_rows - a.num_heavy - a.short_rows;  // the short rows follow
     const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
     const bool live = pos < narrow;  // dead lanes still join the shuffle
     const int glane = lane & ((1 << a.log2g) - 1);
@@ -941,7 +942,7 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
     constexpr int C = Chunk32<T>::C;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t narrow = a.num_rows - a.num_heavy - a.short_rows;  // the short rows follow
     const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
     const bool live = pos < narrow;  // dead lanes still join the shuffle
     const int glane = lane & ((1 << a.log2g) - 1);
@@ -1009,19 +1010,77 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
     }
 }
 
+// The short narrow rows of the entry kernels: the last short_rows narrow positions, which hold
+// at most one quad each, walked with one entry slot.  A row's W chunk lanes each add their
+// 32-byte chunk of all the row's entries, left to right, so a warp covers 32 / W rows, twice as
+// many as entry_rows, and a level of short rows needs half the CTAs.  The codes load before the
+// wait; a longer list is still summed in full (one quad ahead, as entry_rows).
 template <typename T, int INIT, bool UPONLY>
-__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks) {
-    pdl_trigger();
-    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, blockIdx.x);
-    else entry_rows_pre<T, INIT, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+__device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t block) {
+    using Ch = typename Chunk32<T>::type;
+    constexpr int C = Chunk32<T>::C;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int log2w = a.log2g - 1;
+    const int64_t narrow = a.num_rows - a.num_heavy;
+    const int64_t pos = narrow - a.short_rows + ((block * kNarrowWarps + warp) << (5 - log2w)) + (lane >> log2w);
+    const bool live = pos < narrow;
+    const int w = lane & ((1 << log2w) - 1);
+    int32_t q0 = 0, q1 = 0;
+    int64_t row = 0;
+    const uint4* codes4 = reinterpret_cast<const uint4*>(a.entries);
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
+    uint4 cur = null4;
+    if (live) {
+        q0 = __ldg(a.row_ptr + pos) >> 2;
+        q1 = __ldg(a.row_ptr + pos + 1) >> 2;
+        row = level_row(a, pos);
+        if (q0 < q1) cur = __ldg(codes4 + q0);  // static list: before the wait
+    }
+    pdl_wait();
+    if (!live) return;  // no shuffles below
+    const int c = w * C;
+    Ch acc = zero_pack<T, C>();
+    for (int32_t q = q0; q < q1; ++q) {
+        const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
+        const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
+#pragma unroll
+        for (int u = 0; u < 4; u += 2) {  // two fetches in flight, as in the two-slot walk
+            bool ok0, ok1;
+            const T* p0 = lean_source<T, UPONLY>(a, code[u], ok0);
+            const T* p1 = lean_source<T, UPONLY>(a, code[u + 1], ok1);
+            const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
+            const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+            add_into(acc, v0);
+            add_into(acc, v1);
+        }
+        cur = nxt;
+    }
+    Ch out = init_value<T, C, INIT>(a, row, c);
+    add_into(out, acc);
+    st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
 }
 
-// narrow_variant 13: heavy rows (lean walk) first, then the entry-parallel narrow rows.
+// narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (lean walk), the next
+// long_blocks the two-slot narrow rows, the rest the short rows.
 template <typename T, int INIT, bool UPONLY>
-__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks) {
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
-    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, blockIdx.x);
-    else entry_rows<T, INIT, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+    const int64_t b = blockIdx.x;
+    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
+}
+
+// narrow_variant 13: as 14 with entry_rows for the two-slot narrow rows.
+template <typename T, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
+    pdl_trigger();
+    const int64_t b = blockIdx.x;
+    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows<T, INIT, UPONLY>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
@@ -2246,14 +2305,18 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         if (shape) {
             constexpr int rows_per_cta = kWarpRowThreads / 32;
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
-            const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
-            const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + kNarrowWarps - 1) / kNarrowWarps));
+            const int log2w = la.log2g - 1;  // one entry slot: W = G / 2 lanes per short row
+            const int64_t long_rows = narrow - la.short_rows;
+            const int64_t long_warps = (long_rows + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+            const int64_t short_warps = (la.short_rows + (32 >> log2w) - 1) >> (5 - log2w);
+            const int64_t long_blocks = (long_warps + kNarrowWarps - 1) / kNarrowWarps;
+            const dim3 grid(static_cast<unsigned>(heavy_blocks + long_blocks + (short_warps + kNarrowWarps - 1) / kNarrowWarps));
             if (variant == 13) {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks));
+                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
+                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
             } else {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, true>, la, heavy_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, false>, la, heavy_blocks));
+                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
+                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
             }
             GRG_LAUNCH_CHECK("level_entry_kernel");
             return GRG_B200_OK;
@@ -2499,6 +2562,10 @@ int build_level_args(const grg_b200_traverse_args* a, const Shape& sh, const grg
     if (L->list_align == 4 && (L->off_entries % 16) != 0) return fail(GRG_B200_ERR_INVALID, "padded lists must start 16-byte aligned");
     la.list_align = L->list_align;
     la.num_heavy = L->num_heavy;
+    if (L->short_rows < 0 || L->short_rows > L->num_rows - L->num_heavy)
+        return fail(GRG_B200_ERR_INVALID, "short_rows %lld outside [0, %lld]", (long long)L->short_rows,
+                    (long long)(L->num_rows - L->num_heavy));
+    la.short_rows = L->short_rows;
     la.num_slot_buckets = 0;
     if (L->num_slot_buckets < 0 || L->num_slot_buckets > GRG_B200_MAX_SLOT_BUCKETS)
         return fail(GRG_B200_ERR_INVALID, "num_slot_buckets %d outside [0, %d]", L->num_slot_buckets, GRG_B200_MAX_SLOT_BUCKETS);

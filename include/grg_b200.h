@@ -55,7 +55,7 @@
 extern "C" {
 #endif
 
-#define GRG_B200_ABI_VERSION 13
+#define GRG_B200_ABI_VERSION 14
 
 typedef enum grg_b200_status {
     GRG_B200_OK = 0,
@@ -143,6 +143,11 @@ typedef struct grg_b200_level {
     int64_t slot_pos[GRG_B200_MAX_SLOT_BUCKETS];   /* first processing position of bucket b */
     int64_t slot_entry[GRG_B200_MAX_SLOT_BUCKETS]; /* first entry of bucket b */
     int32_t slot_width[GRG_B200_MAX_SLOT_BUCKETS]; /* entries per row of bucket b, in quads of 4 */
+    int64_t short_rows; /* the last short_rows narrow positions (those ending at num_rows -
+                           num_heavy) hold at most 4 entries each: narrow variants 13 and 14 walk
+                           them with one entry slot, twice the rows per CTA.  A speed hint:
+                           longer lists there still sum correctly.  0 <= short_rows <=
+                           num_rows - num_heavy; 0 for none. */
 } grg_b200_level;
 
 typedef struct grg_b200_ring grg_b200_ring; /* opaque: copy stream + per-slot events */
@@ -218,6 +223,8 @@ typedef struct grg_b200_traverse_args {
                                            vector width, no init, 32-byte aligned buffers;
                                            otherwise as 12); 14: as 13 with the codes of a row's
                                            first 4 quads loaded before the previous level ends.
+                                           13 and 14 walk a level's short_rows with one entry
+                                           slot (each lane adds its chunk of all 4 entries).
                                            11 to 14 fall back to 7 with an
                                            error word, split rows or exact order.  Up level
                                            lists name state rows and null padding only. */

@@ -614,6 +614,43 @@ def test_fused_level_runs_are_bit_identical(synth_artifact, k, fuse):
     np.testing.assert_allclose(results[entries][3], oracle.matmul(x_dn, "down", miss=miss.copy()), rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("k", [8, 16])
+@pytest.mark.parametrize("variant", [13, 14])
+def test_short_row_walk_sums_any_list_length(synth_artifact, variant, k):
+    """The entry-parallel walks take a level's ``short_rows`` (the narrow suffix of lists of at
+    most one quad) with one entry slot.  The count is only a speed hint: as built, with none,
+    and with every narrow row walked that way (lists of several quads included), integer inputs
+    give the oracle's results exactly and real ones agree within 1e-12."""
+    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
+
+    oracle = OracleGRG(synth_artifact)
+    plan = B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=2, narrow_split=0)
+    layout = _layout([synth_artifact], requirements=_req(k=k), pair=B200PlanPair(plan_up=plan, plan_down=plan))
+    for mode in ("built", "none", "all"):
+        rng = np.random.default_rng(900 + k)
+        with B200Runtime(layout, check_bounds=False) as runtime:
+            (grg,) = runtime.grgs
+            levels = runtime._artifacts[0].levels
+            arrays = [levels[d].array for d in levels]
+            if mode == "built":
+                assert any(lv.short_rows > 0 for arr in arrays for lv in arr)
+                assert any(0 < lv.short_rows < lv.num_rows - lv.num_heavy for arr in arrays for lv in arr)
+            for arr in arrays:
+                for lv in arr:
+                    if mode == "none":
+                        lv.short_rows = 0
+                    elif mode == "all":
+                        lv.short_rows = lv.num_rows - lv.num_heavy
+            S, M = grg.num_samples, grg.num_mutations
+            for direction, cols in (("up", S), ("down", M)):
+                xi, xr = _pm1(rng, (k, cols)), rng.standard_normal((k, cols))
+                np.testing.assert_array_equal(grg.matmul(xi, direction), oracle.matmul(xi, direction))
+                np.testing.assert_allclose(grg.matmul(xr, direction), oracle.matmul(xr, direction), rtol=1e-12, atol=1e-9)
+            xd, miss = _pm1(rng, (k, M)), _pm1(rng, (k, M))
+            np.testing.assert_array_equal(grg.matmul(xd, "down", miss=miss.copy()), oracle.matmul(xd, "down", miss=miss.copy()))
+            assert runtime.device_error() == 0
+
+
 @pytest.mark.parametrize("k", [1, 3, 8, 16, 33])
 def test_lean_walks_match_variant_7_and_the_oracle(synth_artifact, k):
     """Narrow variants 11, 12 and 13 (the lean walks, used by launches without a bounds-check

@@ -207,3 +207,6 @@ def test_kernel_shape_options_validate_and_round_trip():
     assert (plan.narrow_variant, plan.persist_ctas, plan.fuse_entries, plan.pdl) == (10, 3, 600_000, False)
     with pytest.raises(ValueError, match="unknown B200Plan field"):
         B200Plan.from_dict({"fuse": 1})
+    assert (B200Plan().heavy_buckets, B200Plan().short_rows) == (False, True)
+    plan = B200Plan.from_dict({"heavy_buckets": True, "short_rows": False})
+    assert (plan.heavy_buckets, plan.short_rows) == (True, False)

@@ -112,3 +112,29 @@ def test_heavy_rows_keep_row_order_unless_bucketed():
     assert list(plain.row_ids[:3]) == [0, 5, 2]  # narrow: 2 and 3 entries (bucket 2) in row order, then 1 entry
     grouped = _finish(0, 0, lengths.size, rows, ids, z, z, 4, heavy_buckets=True)
     assert list(grouped.row_ids[-3:]) == [4, 1, 3]  # 20 entries (bucket 5), then 9 and 5 (bucket 4) in row order
+
+
+def test_short_rows_is_the_suffix_of_one_quad_lists():
+    """``short_rows``: the narrow positions at the end of the narrow range whose padded lists
+    hold at most one quad; with long-first bucketing, at least every narrow row of at most 3
+    entries."""
+    from grg_spmv_b200.backends.b200.structures import _finish
+
+    # threshold 8: row 5 (12 entries) is heavy; narrow lengths 4, 7 (bucket 3), 2, 3 (bucket 2),
+    # 1 (bucket 1), 0
+    lengths = np.asarray([2, 7, 0, 4, 1, 12, 3])
+    rows = np.repeat(np.arange(lengths.size), lengths)
+    ids = np.arange(rows.size)
+    z = np.zeros(rows.size, dtype=np.int64)
+    lv = _finish(0, 0, lengths.size, rows, ids, z, z, 8, pad=True)
+    assert list(lv.row_ids) == [1, 3, 0, 6, 4, 2, 5]
+    assert lv.short_rows() == 5  # rows 3 (4 entries: one quad, after its bucket's 7), 0, 6, 4, 2
+    assert _finish(0, 0, lengths.size, rows, ids, z, z, 8, pad=False).short_rows() == 0  # unpadded
+    # short-first order: the last bucket holds rows 1 (7 entries) and 3 (4), in row order
+    assert _finish(0, 0, lengths.size, rows, ids, z, z, 8, pad=True, long_first=False).short_rows() == 1
+    # every narrow row short; at threshold 0 only the empty row stays narrow
+    one = np.asarray([1, 2, 3, 0])
+    r1 = np.repeat(np.arange(one.size), one)
+    z1 = np.zeros(r1.size, dtype=np.int64)
+    assert _finish(0, 0, one.size, r1, np.arange(r1.size), z1, z1, 8, pad=True).short_rows() == 4
+    assert _finish(0, 0, one.size, r1, np.arange(r1.size), z1, z1, 0, pad=True).short_rows() == 1
