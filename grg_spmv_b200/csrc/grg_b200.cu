@@ -1062,25 +1062,91 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
     st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
 }
 
-// narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (lean walk), the next
-// long_blocks the two-slot narrow rows, the rest the short rows.
-template <typename T, int INIT, bool UPONLY>
+// Heavy rows, one warp each, entry-parallel (heavy_variant 4 with the entry kernels).  The warp
+// is W chunk lanes x 32 / W entry slots (W = k / C): lane (e, w) adds 32-byte chunk w of the
+// row's entries e, e + S, e + 2S, ... (S slots), two fetches in flight, the codes of the next
+// two loaded one round ahead.  A code is decoded by W lanes, not 4 * W / 2 as in the 16-byte
+// walk.  An xor butterfly over the slot bits (fixed order) adds the slots; slot 0 stores.
+template <typename T, int INIT, bool UPONLY, int WPC = kWarpRowThreads / 32>
+__device__ __forceinline__ void entry_heavy_rows(const LevelArgs& a, int64_t block) {
+    using Ch = typename Chunk32<T>::type;
+    constexpr int C = Chunk32<T>::C;
+    const int64_t wrow = block * WPC + (threadIdx.x >> 5);
+    if (wrow >= a.num_heavy) return;  // warp-uniform
+    const int lane = threadIdx.x & 31;
+    const int64_t pos = __ldg(a.heavy_rows + wrow);
+    const int32_t end = __ldg(a.row_ptr + pos + 1);
+    const int32_t begin = __ldg(a.row_ptr + pos);
+    const int64_t row = level_row(a, pos);
+    const int log2w = a.log2g - 1;
+    const int w = lane & ((1 << log2w) - 1);
+    const int slots = 32 >> log2w;
+    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
+    int32_t j = begin + (lane >> log2w);
+    uint32_t c0 = j < end ? __ldg(a.entries + j) : null_code;  // static list: before the wait
+    uint32_t c1 = j + slots < end ? __ldg(a.entries + j + slots) : null_code;
+    pdl_wait();
+    const int c = w * C;
+    Ch acc = zero_pack<T, C>();
+    for (; j < end; j += 2 * slots) {
+        const int32_t jn = j + 2 * slots;
+        const uint32_t n0 = jn < end ? __ldg(a.entries + jn) : null_code;
+        const uint32_t n1 = jn + slots < end ? __ldg(a.entries + jn + slots) : null_code;
+        bool ok0, ok1;
+        const T* p0 = lean_source<T, UPONLY>(a, c0, ok0);
+        const T* p1 = lean_source<T, UPONLY>(a, c1, ok1);
+        const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
+        const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+        add_into(acc, v0);
+        add_into(acc, v1);
+        c0 = n0;
+        c1 = n1;
+    }
+    for (int off = 16; off >= (1 << log2w); off >>= 1) {
+        const Ch other = shfl_xor_pack(acc, off);
+        add_into(acc, other);
+    }
+    if (lane < (1 << log2w)) {  // slot 0
+        Ch out = init_value<T, C, INIT>(a, row, c);
+        add_into(out, acc);
+        st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
+    }
+}
+
+template <typename T, int INIT, bool UPONLY, bool HE>
+__device__ __forceinline__ void entry_heavy(const LevelArgs& a, int64_t block) {
+    if constexpr (HE) entry_heavy_rows<T, INIT, UPONLY>(a, block);
+    else lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, block);
+}
+
+// narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (the 16-byte lean walk, or with
+// HE the entry-parallel one), the next long_blocks the two-slot narrow rows, the rest the short
+// rows.
+template <typename T, int INIT, bool UPONLY, bool HE>
 __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
     const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
+    if (b < heavy_blocks) entry_heavy<T, INIT, UPONLY, HE>(a, b);
     else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY>(a, b - heavy_blocks);
     else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 13: as 14 with entry_rows for the two-slot narrow rows.
-template <typename T, int INIT, bool UPONLY>
+template <typename T, int INIT, bool UPONLY, bool HE>
 __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
     const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
+    if (b < heavy_blocks) entry_heavy<T, INIT, UPONLY, HE>(a, b);
     else if (b < heavy_blocks + long_blocks) entry_rows<T, INIT, UPONLY>(a, b - heavy_blocks);
     else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
+}
+
+// All-heavy levels under narrow_variant 13 / 14 with heavy_variant 4: the entry-parallel heavy
+// walk alone, 5 CTAs per SM like the entry kernels.
+template <typename T, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kWarpRowThreads, 5) level_entry_warp_kernel(LevelArgs a) {
+    pdl_trigger();
+    entry_heavy_rows<T, INIT, UPONLY>(a, blockIdx.x);
 }
 
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
@@ -2194,7 +2260,7 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
     if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
-    if (a->heavy_variant < 0 || a->heavy_variant > 3) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 3]", a->heavy_variant);
+    if (a->heavy_variant < 0 || a->heavy_variant > 4) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 4]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
     if (a->persist_ctas < 0) return fail(GRG_B200_ERR_INVALID, "persist_ctas must be >= 0, got %d", a->persist_ctas);
     if (a->fuse_entries < 0) return fail(GRG_B200_ERR_INVALID, "fuse_entries must be >= 0, got %lld", (long long)a->fuse_entries);
@@ -2292,16 +2358,28 @@ template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, int persist_ctas, bool pdl,
                        cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    // the lean walks (11, 12) serve launches without an error word and without row splits;
+    // heavy_variant 4 is the entry-parallel heavy walk of the entry kernels; elsewhere it is 2
+    const bool heavy_entry = heavy_variant == 4;
+    if (heavy_entry) heavy_variant = 2;
+    // the lean walks (11 to 14) serve launches without an error word and without row splits;
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
     if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
-        const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
-                           (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
-                           (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
-                           (!la.use_miss || aligned(la.miss, 32));
+        const bool entry_shape = lean && V == C / 2 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
+                                 (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
+                                 (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
+                                 (!la.use_miss || aligned(la.miss, 32));
+        const bool shape = entry_shape && narrow > 0;
+        if (entry_shape && heavy_entry && narrow == 0 && la.num_heavy > 0) {
+            constexpr int rows_per_cta = kWarpRowThreads / 32;
+            const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
+            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_entry_warp_kernel<T, 0, true>, la));
+            else GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_entry_warp_kernel<T, 0, false>, la));
+            GRG_LAUNCH_CHECK("level_entry_warp_kernel");
+            return GRG_B200_OK;
+        }
         if (shape) {
             constexpr int rows_per_cta = kWarpRowThreads / 32;
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
@@ -2311,13 +2389,15 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
             const int64_t short_warps = (la.short_rows + (32 >> log2w) - 1) >> (5 - log2w);
             const int64_t long_blocks = (long_warps + kNarrowWarps - 1) / kNarrowWarps;
             const dim3 grid(static_cast<unsigned>(heavy_blocks + long_blocks + (short_warps + kNarrowWarps - 1) / kNarrowWarps));
+#define GRG_ENTRY(KERNEL, HE)                                                                                                  \
+    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, true, HE>, la, heavy_blocks, long_blocks));  \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, false, HE>, la, heavy_blocks, long_blocks));
             if (variant == 13) {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
+                if (heavy_entry) { GRG_ENTRY(level_entry_kernel, true) } else { GRG_ENTRY(level_entry_kernel, false) }
             } else {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
+                if (heavy_entry) { GRG_ENTRY(level_entry_pre_kernel, true) } else { GRG_ENTRY(level_entry_pre_kernel, false) }
             }
+#undef GRG_ENTRY
             GRG_LAUNCH_CHECK("level_entry_kernel");
             return GRG_B200_OK;
         }

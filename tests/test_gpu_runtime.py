@@ -614,17 +614,19 @@ def test_fused_level_runs_are_bit_identical(synth_artifact, k, fuse):
     np.testing.assert_allclose(results[entries][3], oracle.matmul(x_dn, "down", miss=miss.copy()), rtol=1e-12, atol=1e-9)
 
 
+@pytest.mark.parametrize("heavy", [2, 4])
 @pytest.mark.parametrize("k", [8, 16])
 @pytest.mark.parametrize("variant", [13, 14])
-def test_short_row_walk_sums_any_list_length(synth_artifact, variant, k):
+def test_short_row_walk_sums_any_list_length(synth_artifact, variant, k, heavy):
     """The entry-parallel walks take a level's ``short_rows`` (the narrow suffix of lists of at
     most one quad) with one entry slot.  The count is only a speed hint: as built, with none,
     and with every narrow row walked that way (lists of several quads included), integer inputs
-    give the oracle's results exactly and real ones agree within 1e-12."""
+    give the oracle's results exactly and real ones agree within 1e-12, with either heavy walk
+    (2: quads of 16-byte loads; 4: entry-parallel 32-byte chunks)."""
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
 
     oracle = OracleGRG(synth_artifact)
-    plan = B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=2, narrow_split=0)
+    plan = B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=heavy, narrow_split=0)
     layout = _layout([synth_artifact], requirements=_req(k=k), pair=B200PlanPair(plan_up=plan, plan_down=plan))
     for mode in ("built", "none", "all"):
         rng = np.random.default_rng(900 + k)
