@@ -635,6 +635,7 @@ def test_short_row_walk_sums_any_list_length(synth_artifact, variant, k, heavy):
             levels = runtime._artifacts[0].levels
             arrays = [levels[d].array for d in levels]
             if mode == "built":
+                assert any(lv.num_heavy > 0 for arr in arrays for lv in arr)
                 assert any(lv.short_rows > 0 for arr in arrays for lv in arr)
                 assert any(0 < lv.short_rows < lv.num_rows - lv.num_heavy for arr in arrays for lv in arr)
             for arr in arrays:
