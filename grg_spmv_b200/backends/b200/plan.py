@@ -97,6 +97,10 @@ class B200Plan:
     power-of-two length buckets.  Off by default: heavy rows then stay in row order (locality
     order for down), so rows that share source rows run together.  On config 2 at k = 8 this
     is what lets down level 0 read each parent row from DRAM about once.
+    ``early_sources``: with programmatic dependent launch and resident levels, chain a
+    traversal's level launches: each lets the next start only after its own wait, and from
+    the second level on the variant-14 walks add every source older than the previous launch
+    before waiting, so they overlap the previous level's tail (``GRG_B200_LAUNCH_EARLY``).
     ``short_rows``: let narrow variants 13 and 14 walk each level's narrow suffix of lists of at
     most one quad (4 entries) with one entry slot, so a CTA covers twice the rows there.  On
     by default; most rows of the upper down levels are that short.
@@ -123,6 +127,7 @@ class B200Plan:
     fuse_entries: int = 0
     heavy_buckets: bool = False
     short_rows: bool = True
+    early_sources: bool = False
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -178,7 +183,7 @@ class B200Plan:
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
                    "heavy_variant", "long_first", "narrow_split", "schedule", "slots", "pdl", "persist_ctas", "fuse_entries",
-                   "heavy_buckets", "short_rows"}
+                   "heavy_buckets", "short_rows", "early_sources"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -191,7 +196,8 @@ class B200Plan:
                    schedule=str(value.get("schedule", "levels")), slots=bool(value.get("slots", False)),
                    pdl=None if value.get("pdl") is None else bool(value.get("pdl")),
                    persist_ctas=int(value.get("persist_ctas", 0)), fuse_entries=int(value.get("fuse_entries", 0)),
-                   heavy_buckets=bool(value.get("heavy_buckets", False)), short_rows=bool(value.get("short_rows", True)))
+                   heavy_buckets=bool(value.get("heavy_buckets", False)), short_rows=bool(value.get("short_rows", True)),
+                   early_sources=bool(value.get("early_sources", False)))
 
 
 @dataclass(frozen=True)

@@ -266,6 +266,14 @@ typedef struct grg_b200_traverse_args {
  * level lists until the hardware reports that kernel complete, and so overlaps the launch
  * gap.  Ignored when any level is streamed. */
 #define GRG_B200_LAUNCH_PDL 1
+/* With GRG_B200_LAUNCH_PDL and resident levels: chain the level launches.  Each level kernel
+ * lets the next launch start only after its own wait on the previous one, so while launch i
+ * runs, launches up to i - 2 are complete; from the second level launch on, the narrow
+ * variant 14 walks (and the heavy walk of all-heavy levels) add every source that the
+ * previous launch does not write before their wait, and only the rest after it.  Lists hold
+ * a row's sources by level, the previous launch's last, as the list builders write them.
+ * Other kernels run unchained. */
+#define GRG_B200_LAUNCH_EARLY 2
 
 /*
  * GRG_B200_SCHEDULE_LEVELS: one launch per level (each level waits for the previous one).
