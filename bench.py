@@ -88,8 +88,6 @@ def parse_args():
                    help="heavy-row kernel: 0 CTA per row, 1 warp per row, 2 warp per row fused into the narrow launch")
     p.add_argument("--short-first", action="store_true", help="process length buckets shortest first")
     p.add_argument("--heavy-buckets", action="store_true", help="also group heavy rows by length (default: row order)")
-    p.add_argument("--early-sources", action="store_true",
-                   help="chain the level launches and gather older sources before each wait")
     p.add_argument("--no-short-rows", action="store_true",
                    help="walk the one-quad narrow rows with two entry slots like the rest (default: one slot)")
     p.add_argument("--slots", choices=["none", "up", "down", "both"], default="none",
@@ -321,8 +319,6 @@ def run_b200(args) -> None:
         extra["heavy_buckets"] = True
     if args.no_short_rows:
         extra["short_rows"] = False
-    if args.early_sources:
-        extra["early_sources"] = True
     if args.pdl != "auto":
         extra["pdl"] = args.pdl == "on"
     if args.narrow_split is not None:
@@ -469,7 +465,7 @@ def run_b200(args) -> None:
                 if pair.plan_down.schedule == "dataflow":
                     level_launches += 3 if name == "up" else 2  # sentinel fill (+ seed) + dataflow kernel + output
                 else:
-                    fused = op._args.heavy_variant in (2, 4) and op._args.narrow_variant >= 6 and not op._args.exact_order
+                    fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                     lv_arr = runtime._artifacts[0].levels[op._spec.direction].array
                     level_launches += traversal_level_launches(lv_arr, fused, int(op._args.fuse_entries)) + (2 if name == "up" else 1)
                 lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
@@ -487,7 +483,7 @@ def run_b200(args) -> None:
             for i in range(levels.count):
                 nat.check(lib, lib.grg_b200_run_level(ctypes.byref(args_c), ctypes.byref(levels.array[i]),
                                                       ctypes.c_void_p(stream.cuda_stream)), "run_level")
-                fused = op._args.heavy_variant in (2, 4) and op._args.narrow_variant >= 6 and not op._args.exact_order
+                fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                 lv = levels.array[i]
                 level_launches += 1 + (1 if 0 < lv.num_heavy < lv.num_rows and not fused else 0)
             b.record(stream)
@@ -699,7 +695,7 @@ def run_b200(args) -> None:
                        "num_levels": scan.num_levels, "exact_order": bool(args.exact_order),
                        "heavy_threshold": pair.plan_down.heavy_threshold, "narrow_variant": narrow_used,
                        "cuda_graphs": not args.no_graphs, "balance": pair.plan_down.balance, "pad_lists": pair.plan_down.pad_lists,
-                       "long_first": pair.plan_down.long_first, "heavy_buckets": pair.plan_down.heavy_buckets, "short_rows": pair.plan_down.short_rows, "early_sources": pair.plan_down.early_sources, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
+                       "long_first": pair.plan_down.long_first, "heavy_buckets": pair.plan_down.heavy_buckets, "short_rows": pair.plan_down.short_rows, "slots": {"up": pair.plan_up.slots, "down": pair.plan_down.slots}, "pdl": pair.plan_down.resolve_pdl(k), "narrow_split": pair.plan_down.narrow_split, "fuse_entries": pair.plan_down.fuse_entries,
                        "schedule": pair.plan_down.schedule,
                        "heavy_variant": heavy_used, "autotuned_variants": tuned,
                        "row_order": {"up": "locality" if pair.plan_up.locality(Direction.UP) else "natural",

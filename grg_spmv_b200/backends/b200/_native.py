@@ -30,7 +30,6 @@ OK, ERR_INVALID, ERR_CUDA, ERR_UNSUPPORTED = 0, 1, 2, 3
 F64, F32, MIXED = 0, 1, 2
 MAX_SLOT_BUCKETS = 8
 LAUNCH_PDL = 1
-LAUNCH_EARLY = 2
 SCHEDULE_LEVELS, SCHEDULE_DATAFLOW = 0, 1
 DEVICE_WAIT_TIMEOUT = 6
 UP, DOWN = 0, 1

@@ -73,10 +73,8 @@ class B200Plan:
     ``heavy_variant``).
     ``pad_lists``: pad every gather list to a multiple of 4 entries (needed by variant 6).
     ``heavy_variant``: heavy rows one CTA each (0), one warp each (1), or one warp each inside
-    the narrow-row launch (2, with ``narrow_variant`` 6 or 7); 3 as 1 with 32 rows per CTA;
-    4 as 2 with the entry-parallel walk of 32-byte chunks under ``narrow_variant`` 13 and 14
-    (elsewhere as 2).  None picks 2 with the padded variants and otherwise 1 for k <= 16, 0
-    above.  Exact order always uses CTAs.
+    the narrow-row launch (2, with ``narrow_variant`` 6 or 7); None picks 2 with the padded
+    variants and otherwise 1 for k <= 16, 0 above.  Exact order always uses CTAs.
     ``long_first``: with ``balance``, the longest length bucket is processed first.
     ``pdl``: launch the level, seed and output kernels with programmatic dependent launch
     (each overlaps the end of the previous one; ignored when levels are streamed).  None turns
@@ -97,10 +95,6 @@ class B200Plan:
     power-of-two length buckets.  Off by default: heavy rows then stay in row order (locality
     order for down), so rows that share source rows run together.  On config 2 at k = 8 this
     is what lets down level 0 read each parent row from DRAM about once.
-    ``early_sources``: with programmatic dependent launch and resident levels, chain a
-    traversal's level launches: each lets the next start only after its own wait, and from
-    the second level on the variant-14 walks add every source older than the previous launch
-    before waiting, so they overlap the previous level's tail (``GRG_B200_LAUNCH_EARLY``).
     ``short_rows``: let narrow variants 13 and 14 walk each level's narrow suffix of lists of at
     most one quad (4 entries) with one entry slot, so a CTA covers twice the rows there.  On
     by default; most rows of the upper down levels are that short.
@@ -127,7 +121,6 @@ class B200Plan:
     fuse_entries: int = 0
     heavy_buckets: bool = False
     short_rows: bool = True
-    early_sources: bool = False
 
     def __post_init__(self) -> None:
         if int(self.heavy_threshold) < 1:
@@ -138,8 +131,8 @@ class B200Plan:
             raise ValueError(f"narrow_variant must be in [0, {nat.NARROW_VARIANTS}), got {self.narrow_variant}")
         if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
             raise ValueError(f"narrow_variants 6-{nat.NARROW_VARIANTS - 1} read padded gather lists; they need pad_lists=True")
-        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3, 4):
-            raise ValueError(f"heavy_variant must be 0 to 4, got {self.heavy_variant}")
+        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3):
+            raise ValueError(f"heavy_variant must be 0, 1, 2 or 3, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:
             raise ValueError(f"narrow_split must be in [-1, 3], got {self.narrow_split}")
         if self.schedule not in ("levels", "dataflow"):
@@ -183,7 +176,7 @@ class B200Plan:
     def from_dict(cls, value: Mapping[str, object]) -> "B200Plan":
         allowed = {"exact_order", "heavy_threshold", "row_order", "narrow_variant", "balance", "autotune", "pad_lists",
                    "heavy_variant", "long_first", "narrow_split", "schedule", "slots", "pdl", "persist_ctas", "fuse_entries",
-                   "heavy_buckets", "short_rows", "early_sources"}
+                   "heavy_buckets", "short_rows"}
         extra = sorted(set(value) - allowed)
         if extra:
             raise ValueError(f"unknown B200Plan field(s): {extra}")
@@ -196,8 +189,7 @@ class B200Plan:
                    schedule=str(value.get("schedule", "levels")), slots=bool(value.get("slots", False)),
                    pdl=None if value.get("pdl") is None else bool(value.get("pdl")),
                    persist_ctas=int(value.get("persist_ctas", 0)), fuse_entries=int(value.get("fuse_entries", 0)),
-                   heavy_buckets=bool(value.get("heavy_buckets", False)), short_rows=bool(value.get("short_rows", True)),
-                   early_sources=bool(value.get("early_sources", False)))
+                   heavy_buckets=bool(value.get("heavy_buckets", False)), short_rows=bool(value.get("short_rows", True)))
 
 
 @dataclass(frozen=True)

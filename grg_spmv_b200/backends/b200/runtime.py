@@ -509,7 +509,7 @@ class B200Runtime:
         a.narrow_split = int(plan.narrow_split)
         a.persist_ctas = int(plan.persist_ctas)
         a.fuse_entries = int(plan.fuse_entries)
-        a.launch_flags = (nat.LAUNCH_PDL | (nat.LAUNCH_EARLY if plan.early_sources else 0)) if plan.resolve_pdl(k) else 0
+        a.launch_flags = nat.LAUNCH_PDL if plan.resolve_pdl(k) else 0
         a.schedule = nat.SCHEDULE_DATAFLOW if plan.schedule == "dataflow" else nat.SCHEDULE_LEVELS
         a.dataflow_sync = _ptr(self._df_sync if df_sync is None else df_sync)
         return a

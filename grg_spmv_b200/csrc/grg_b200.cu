@@ -217,14 +217,6 @@ struct LevelArgs {
     const void* miss_lo;
     int32_t up;  // an up level: its lists name state rows (and null padding) only
     int64_t short_rows;  // entry kernels: the last short_rows narrow positions take one entry slot
-    // Chained traversal (GRG_B200_LAUNCH_EARLY): a level launch lets the next one start only
-    // after its own wait on the previous launch, so while launch i runs, launches up to i - 2
-    // are complete.  With `early`, the walks add every source outside the rows the previous
-    // launch writes, [late_lo, late_lo + late_n), before their wait.
-    int32_t chain;
-    int32_t early;
-    uint32_t late_lo;
-    uint32_t late_n;
 };
 
 enum DeviceError : int32_t {
@@ -247,20 +239,6 @@ __device__ __forceinline__ void report(int32_t* err, int32_t code) {
 // kernel launch once every CTA of this grid has started.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
-
-// Level kernels that take part in a chained traversal: the trigger moves from the kernel's
-// start to just after its wait, so the next launch starts only once the previous one is done.
-__device__ __forceinline__ void pdl_start(const LevelArgs& a) {
-    if (!a.chain) pdl_trigger();
-}
-__device__ __forceinline__ void pdl_wait_chain(const LevelArgs& a) {
-    pdl_wait();
-    if (a.chain) pdl_trigger();
-}
-// A source that the previous launch writes (only state rows can be): it waits for pdl_wait.
-__device__ __forceinline__ bool late_src(const LevelArgs& a, uint32_t code) {
-    return ((code >> GRG_B200_SRC_SHIFT) & GRG_B200_SRC_MASK) == GRG_B200_SRC_STATE && (code & GRG_B200_ID_MASK) - a.late_lo < a.late_n;
-}
 
 template <typename T, int V, int INIT>
 __device__ __forceinline__ Pack<T, V> init_value(const LevelArgs& a, int64_t row, int64_t c) {
@@ -820,7 +798,7 @@ __device__ __forceinline__ void lean_rows(const LevelArgs& a, int64_t block) {
 }
 
 // Heavy rows, one warp each, as warp_heavy_rows (padded lists) with the lean decode.
-template <typename T, int V, int INIT, bool UPONLY, bool EARLY = false, int WPC = kWarpRowThreads / 32>
+template <typename T, int V, int INIT, bool UPONLY, int WPC = kWarpRowThreads / 32>
 __device__ __forceinline__ void lean_heavy_rows(const LevelArgs& a, int64_t block) {
     const int64_t w = block * WPC + (threadIdx.x >> 5);
     if (w >= a.num_heavy) return;  // warp-uniform
@@ -829,6 +807,7 @@ __device__ __forceinline__ void lean_heavy_rows(const LevelArgs& a, int64_t bloc
     const int32_t q1 = __ldg(a.row_ptr + pos + 1) >> 2;
     const int32_t qs = __ldg(a.row_ptr + pos) >> 2;
     const int64_t row = level_row(a, pos);
+    pdl_wait();
     const int g_lanes = 1 << a.log2g;
     const int groups = 32 >> a.log2g;
     const int glane = lane32 & (g_lanes - 1);
@@ -839,49 +818,13 @@ __device__ __forceinline__ void lean_heavy_rows(const LevelArgs& a, int64_t bloc
     const uint4 null4 = make_uint4(null_code, null_code, null_code, null_code);
     const int step = V << a.log2g;
     const int k = static_cast<int>(a.k);
-    // Chained traversal, one pass over the columns: the group adds its quads up to the first
-    // source the previous launch writes before the wait (lists hold those sources last), and
-    // keeps that quad's remaining codes for after it.
-    const bool pre = EARLY && a.early && step >= k;
-    int32_t q = qs + grp;
-    uint4 cur = null4;
-    Pack<T, V> early_part = zero_pack<T, V>();
-    if (EARLY && pre && glane * V < k) {
-        const int c = glane * V;
-        cur = q < q1 ? __ldg(codes4 + q) : null4;
-        for (; q < q1; q += groups) {
-            const uint4 nxt = q + groups < q1 ? __ldg(codes4 + q + groups) : null4;
-            const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
-            bool late[4];
-            late[0] = late_src(a, code[0]);
-#pragma unroll
-            for (int u = 1; u < 4; ++u) late[u] = late[u - 1] || late_src(a, code[u]);
-            Pack<T, V> val[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                bool ok;
-                const T* p = lean_source<T, UPONLY>(a, code[u], ok);
-                val[u] = ok && !late[u] ? ld_ro<T, V>(p + c) : zero_pack<T, V>();
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) add_into(early_part, val[u]);
-            if (late[3]) {
-                cur = make_uint4(late[0] ? code[0] : null_code, late[1] ? code[1] : null_code, late[2] ? code[2] : null_code, code[3]);
-                break;
-            }
-            cur = nxt;
-        }
-    }
-    pdl_wait_chain(a);
     for (int base = 0; base < k; base += step) {  // uniform trip count across the warp
         const int c = base + glane * V;
         const bool active = c < k;
-        Pack<T, V> part = early_part;  // zero unless `pre` (then this is the only pass)
+        Pack<T, V> part = zero_pack<T, V>();
         if (active) {
-            if (!pre) {
-                q = qs + grp;
-                cur = q < q1 ? __ldg(codes4 + q) : null4;
-            }
+            int32_t q = qs + grp;
+            uint4 cur = q < q1 ? __ldg(codes4 + q) : null4;
             for (; q < q1; q += groups) {
                 const uint4 nxt = q + groups < q1 ? __ldg(codes4 + q + groups) : null4;
                 const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
@@ -961,7 +904,7 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
         row = level_row(a, pos);
         if (q0 < q1) cur = __ldg(codes4 + q0);  // static list: before the wait
     }
-    pdl_wait_chain(a);
+    pdl_wait();
     const int c = w * C;
     Ch acc = zero_pack<T, C>();
     for (int32_t q = q0; q < q1; ++q) {
@@ -993,7 +936,7 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
 // rest one round ahead, as entry_rows does.
 constexpr int kPreQuads = 4;
 
-template <typename T, int INIT, bool UPONLY, bool EARLY>
+template <typename T, int INIT, bool UPONLY>
 __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block) {
     using Ch = typename Chunk32<T>::type;
     constexpr int C = Chunk32<T>::C;
@@ -1026,36 +969,12 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
             }
         }
     }
+    pdl_wait();
     const int c = w * C;
     Ch acc = zero_pack<T, C>();
-    int32_t qs = q0;  // the preloaded quads from qs on are added after the wait
-    if (EARLY && a.early && live) {  // chained traversal: this lane's codes up to the first late source
-        bool go = true;
-#pragma unroll
-        for (int j = 0; j < kPreQuads; ++j) {
-            if (go && q0 + j < q1) {
-                const bool late0 = late_src(a, pre0[j]);
-                const bool late1 = late0 || late_src(a, pre1[j]);
-                bool ok0, ok1;
-                const T* p0 = lean_source<T, UPONLY>(a, pre0[j], ok0);
-                const T* p1 = lean_source<T, UPONLY>(a, pre1[j], ok1);
-                const Ch v0 = ok0 && !late0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-                const Ch v1 = ok1 && !late1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
-                add_into(acc, v0);
-                add_into(acc, v1);
-                if (late1) {
-                    go = false;
-                    if (!late0) pre0[j] = null_code;  // added already
-                } else {
-                    qs = q0 + j + 1;
-                }
-            }
-        }
-    }
-    pdl_wait_chain(a);
 #pragma unroll
     for (int j = 0; j < kPreQuads; ++j) {
-        if (q0 + j < q1 && q0 + j >= qs) {
+        if (q0 + j < q1) {
             bool ok0, ok1;
             const T* p0 = lean_source<T, UPONLY>(a, pre0[j], ok0);
             const T* p1 = lean_source<T, UPONLY>(a, pre1[j], ok1);
@@ -1096,7 +1015,7 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
 // 32-byte chunk of all the row's entries, left to right, so a warp covers 32 / W rows, twice as
 // many as entry_rows, and a level of short rows needs half the CTAs.  The codes load before the
 // wait; a longer list is still summed in full (one quad ahead, as entry_rows).
-template <typename T, int INIT, bool UPONLY, bool EARLY>
+template <typename T, int INIT, bool UPONLY>
 __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t block) {
     using Ch = typename Chunk32<T>::type;
     constexpr int C = Chunk32<T>::C;
@@ -1119,32 +1038,10 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
         row = level_row(a, pos);
         if (q0 < q1) cur = __ldg(codes4 + q0);  // static list: before the wait
     }
+    pdl_wait();
+    if (!live) return;  // no shuffles below
     const int c = w * C;
     Ch acc = zero_pack<T, C>();
-    if (EARLY && a.early && live) {  // chained traversal: the first quad's codes up to the first late source
-        uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
-        bool go = true;
-#pragma unroll
-        for (int u = 0; u < 4; u += 2) {
-            if (go) {
-                const bool late0 = late_src(a, code[u]);
-                const bool late1 = late0 || late_src(a, code[u + 1]);
-                bool ok0, ok1;
-                const T* p0 = lean_source<T, UPONLY>(a, code[u], ok0);
-                const T* p1 = lean_source<T, UPONLY>(a, code[u + 1], ok1);
-                const Ch v0 = ok0 && !late0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-                const Ch v1 = ok1 && !late1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
-                add_into(acc, v0);
-                add_into(acc, v1);
-                if (!late0) code[u] = null_code;  // added already
-                if (!late1) code[u + 1] = null_code;
-                go = !late1;
-            }
-        }
-        cur = make_uint4(code[0], code[1], code[2], code[3]);
-    }
-    pdl_wait_chain(a);
-    if (!live) return;  // no shuffles below
     for (int32_t q = q0; q < q1; ++q) {
         const uint4 nxt = q + 1 < q1 ? __ldg(codes4 + q + 1) : null4;
         const uint32_t code[4] = {cur.x, cur.y, cur.z, cur.w};
@@ -1165,91 +1062,25 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
     st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
 }
 
-// Heavy rows, one warp each, entry-parallel (heavy_variant 4 with the entry kernels).  The warp
-// is W chunk lanes x 32 / W entry slots (W = k / C): lane (e, w) adds 32-byte chunk w of the
-// row's entries e, e + S, e + 2S, ... (S slots), two fetches in flight, the codes of the next
-// two loaded one round ahead.  A code is decoded by W lanes, not 4 * W / 2 as in the 16-byte
-// walk.  An xor butterfly over the slot bits (fixed order) adds the slots; slot 0 stores.
-template <typename T, int INIT, bool UPONLY, int WPC = kWarpRowThreads / 32>
-__device__ __forceinline__ void entry_heavy_rows(const LevelArgs& a, int64_t block) {
-    using Ch = typename Chunk32<T>::type;
-    constexpr int C = Chunk32<T>::C;
-    const int64_t wrow = block * WPC + (threadIdx.x >> 5);
-    if (wrow >= a.num_heavy) return;  // warp-uniform
-    const int lane = threadIdx.x & 31;
-    const int64_t pos = __ldg(a.heavy_rows + wrow);
-    const int32_t end = __ldg(a.row_ptr + pos + 1);
-    const int32_t begin = __ldg(a.row_ptr + pos);
-    const int64_t row = level_row(a, pos);
-    const int log2w = a.log2g - 1;
-    const int w = lane & ((1 << log2w) - 1);
-    const int slots = 32 >> log2w;
-    const uint32_t null_code = GRG_B200_SRC_NULL << GRG_B200_SRC_SHIFT;
-    int32_t j = begin + (lane >> log2w);
-    uint32_t c0 = j < end ? __ldg(a.entries + j) : null_code;  // static list: before the wait
-    uint32_t c1 = j + slots < end ? __ldg(a.entries + j + slots) : null_code;
-    pdl_wait_chain(a);
-    const int c = w * C;
-    Ch acc = zero_pack<T, C>();
-    for (; j < end; j += 2 * slots) {
-        const int32_t jn = j + 2 * slots;
-        const uint32_t n0 = jn < end ? __ldg(a.entries + jn) : null_code;
-        const uint32_t n1 = jn + slots < end ? __ldg(a.entries + jn + slots) : null_code;
-        bool ok0, ok1;
-        const T* p0 = lean_source<T, UPONLY>(a, c0, ok0);
-        const T* p1 = lean_source<T, UPONLY>(a, c1, ok1);
-        const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-        const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
-        add_into(acc, v0);
-        add_into(acc, v1);
-        c0 = n0;
-        c1 = n1;
-    }
-    for (int off = 16; off >= (1 << log2w); off >>= 1) {
-        const Ch other = shfl_xor_pack(acc, off);
-        add_into(acc, other);
-    }
-    if (lane < (1 << log2w)) {  // slot 0
-        Ch out = init_value<T, C, INIT>(a, row, c);
-        add_into(out, acc);
-        st_pack(static_cast<T*>(a.state) + row * a.ld_state + c, out);
-    }
-}
-
-template <typename T, int INIT, bool UPONLY, bool HE, bool EARLY>
-__device__ __forceinline__ void entry_heavy(const LevelArgs& a, int64_t block) {
-    if constexpr (HE) entry_heavy_rows<T, INIT, UPONLY>(a, block);
-    else lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY, EARLY>(a, block);
-}
-
-// narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (the 16-byte lean walk, or with
-// HE the entry-parallel one), the next long_blocks the two-slot narrow rows, the rest the short
-// rows.
-template <typename T, int INIT, bool UPONLY, bool HE, bool EARLY>
+// narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (lean walk), the next
+// long_blocks the two-slot narrow rows, the rest the short rows.
+template <typename T, int INIT, bool UPONLY>
 __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
-    pdl_start(a);
+    pdl_trigger();
     const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) entry_heavy<T, INIT, UPONLY, HE, EARLY>(a, b);
-    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY, EARLY>(a, b - heavy_blocks);
-    else entry_short_rows<T, INIT, UPONLY, EARLY>(a, b - heavy_blocks - long_blocks);
+    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 13: as 14 with entry_rows for the two-slot narrow rows.
-template <typename T, int INIT, bool UPONLY, bool HE>
-__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
-    pdl_start(a);
-    const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) entry_heavy<T, INIT, UPONLY, HE, false>(a, b);
-    else if (b < heavy_blocks + long_blocks) entry_rows<T, INIT, UPONLY>(a, b - heavy_blocks);
-    else entry_short_rows<T, INIT, UPONLY, false>(a, b - heavy_blocks - long_blocks);
-}
-
-// All-heavy levels under narrow_variant 13 / 14 with heavy_variant 4: the entry-parallel heavy
-// walk alone, 5 CTAs per SM like the entry kernels.
 template <typename T, int INIT, bool UPONLY>
-__global__ void __launch_bounds__(kWarpRowThreads, 5) level_entry_warp_kernel(LevelArgs a) {
-    pdl_start(a);
-    entry_heavy_rows<T, INIT, UPONLY>(a, blockIdx.x);
+__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
+    pdl_trigger();
+    const int64_t b = blockIdx.x;
+    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows<T, INIT, UPONLY>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
@@ -1262,10 +1093,10 @@ __global__ void __launch_bounds__(kNarrowThreads, 5) level_lean_kernel(LevelArgs
 }
 
 // All-heavy levels under narrow_variant 11 / 12: the lean heavy walk alone.
-template <typename T, int V, int INIT, bool UPONLY, bool EARLY = false>
+template <typename T, int V, int INIT, bool UPONLY>
 __global__ void __launch_bounds__(kWarpRowThreads) level_lean_warp_kernel(LevelArgs a) {
-    pdl_start(a);
-    lean_heavy_rows<T, V, INIT, UPONLY, EARLY>(a, blockIdx.x);
+    pdl_trigger();
+    lean_heavy_rows<T, V, INIT, UPONLY>(a, blockIdx.x);
 }
 
 // Narrow rows of padded lists, persistent (narrow_variant 9 and 10).  The narrow CTAs of a
@@ -2363,7 +2194,7 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
     if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
-    if (a->heavy_variant < 0 || a->heavy_variant > 4) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 4]", a->heavy_variant);
+    if (a->heavy_variant < 0 || a->heavy_variant > 3) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 3]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
     if (a->persist_ctas < 0) return fail(GRG_B200_ERR_INVALID, "persist_ctas must be >= 0, got %d", a->persist_ctas);
     if (a->fuse_entries < 0) return fail(GRG_B200_ERR_INVALID, "fuse_entries must be >= 0, got %lld", (long long)a->fuse_entries);
@@ -2457,56 +2288,21 @@ int launch_persist(const LevelArgs& la, int init_mode, int variant, int64_t heav
     return GRG_B200_OK;
 }
 
-// A level launch's place in a chained traversal: `chain` to trigger after the wait, `early`
-// when the launch before it was chained too (so launches up to two back are complete), and
-// the node rows [late_lo, late_lo + late_n) that the previous launch writes.
-struct ChainInfo {
-    bool chain = false;
-    bool early = false;
-    uint32_t late_lo = 0;
-    uint32_t late_n = 0;
-};
-
 template <typename T, int V>
-int launch_level_typed(const LevelArgs& la_in, int init_mode, bool exact, int variant, int heavy_variant, int persist_ctas, bool pdl,
-                       cudaStream_t s, const ChainInfo& ci = ChainInfo{}, bool* chained = nullptr) {
-    // the entry kernels and the lean heavy walks of all-heavy levels take part in a chained
-    // traversal; every other kernel starts as before and reports that it did not
-    LevelArgs la = la_in;
-    if (chained) *chained = false;
-    const auto chain_in = [&](bool early_walk) {
-        la.chain = ci.chain && pdl;
-        la.early = la.chain && ci.early && early_walk;
-        la.late_lo = ci.late_lo;
-        la.late_n = ci.late_n;
-        if (chained) *chained = la.chain;
-    };
+int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, int persist_ctas, bool pdl,
+                       cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    // heavy_variant 4 is the entry-parallel heavy walk of the entry kernels; elsewhere it is 2
-    const bool heavy_entry = heavy_variant == 4;
-    if (heavy_entry) heavy_variant = 2;
-    // the lean walks (11 to 14) serve launches without an error word and without row splits;
+    // the lean walks (11, 12) serve launches without an error word and without row splits;
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
     if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
-        const bool entry_shape = lean && V == C / 2 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
-                                 (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
-                                 (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
-                                 (!la.use_miss || aligned(la.miss, 32));
-        const bool shape = entry_shape && narrow > 0;
-        if (entry_shape && heavy_entry && narrow == 0 && la.num_heavy > 0) {
-            chain_in(false);
-            constexpr int rows_per_cta = kWarpRowThreads / 32;
-            const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
-            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_entry_warp_kernel<T, 0, true>, la));
-            else GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_entry_warp_kernel<T, 0, false>, la));
-            GRG_LAUNCH_CHECK("level_entry_warp_kernel");
-            return GRG_B200_OK;
-        }
+        const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
+                           (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
+                           (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
+                           (!la.use_miss || aligned(la.miss, 32));
         if (shape) {
-            chain_in(variant == 14);  // 13 chains without early gathers
             constexpr int rows_per_cta = kWarpRowThreads / 32;
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
             const int log2w = la.log2g - 1;  // one entry slot: W = G / 2 lanes per short row
@@ -2515,17 +2311,13 @@ int launch_level_typed(const LevelArgs& la_in, int init_mode, bool exact, int va
             const int64_t short_warps = (la.short_rows + (32 >> log2w) - 1) >> (5 - log2w);
             const int64_t long_blocks = (long_warps + kNarrowWarps - 1) / kNarrowWarps;
             const dim3 grid(static_cast<unsigned>(heavy_blocks + long_blocks + (short_warps + kNarrowWarps - 1) / kNarrowWarps));
-#define GRG_ENTRY(KERNEL, ...)                                                                                                    \
-    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, true, __VA_ARGS__>, la, heavy_blocks, long_blocks));  \
-    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, false, __VA_ARGS__>, la, heavy_blocks, long_blocks));
             if (variant == 13) {
-                if (heavy_entry) { GRG_ENTRY(level_entry_kernel, true) } else { GRG_ENTRY(level_entry_kernel, false) }
-            } else if (la.early) {
-                if (heavy_entry) { GRG_ENTRY(level_entry_pre_kernel, true, true) } else { GRG_ENTRY(level_entry_pre_kernel, false, true) }
+                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
+                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
             } else {
-                if (heavy_entry) { GRG_ENTRY(level_entry_pre_kernel, true, false) } else { GRG_ENTRY(level_entry_pre_kernel, false, false) }
+                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
+                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
             }
-#undef GRG_ENTRY
             GRG_LAUNCH_CHECK("level_entry_kernel");
             return GRG_B200_OK;
         }
@@ -2549,20 +2341,14 @@ int launch_level_typed(const LevelArgs& la_in, int init_mode, bool exact, int va
             return GRG_B200_OK;
         }
         if (lean && narrow == 0 && la.num_heavy > 0) {
-            chain_in(la.log2s == 0);
             constexpr int rows_per_cta = kWarpRowThreads / 32;
             const dim3 grid(static_cast<unsigned>((la.num_heavy + rows_per_cta - 1) / rows_per_cta));
 #define GRG_LEAN_WARP(INIT)                                                                                                            if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_kernel<T, V, INIT, true>, la));                    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_kernel<T, V, INIT, false>, la));
-            if (la.early && init_mode == 0) {  // chained: sources older than the previous launch first
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_kernel<T, V, 0, true, true>, la));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kWarpRowThreads, level_lean_warp_kernel<T, V, 0, false, true>, la));
-            } else {
-                switch (init_mode) {
-                    case 0: GRG_LEAN_WARP(0) break;
-                    case 1: GRG_LEAN_WARP(1) break;
-                    case 2: GRG_LEAN_WARP(2) break;
-                    default: GRG_LEAN_WARP(3) break;
-                }
+            switch (init_mode) {
+                case 0: GRG_LEAN_WARP(0) break;
+                case 1: GRG_LEAN_WARP(1) break;
+                case 2: GRG_LEAN_WARP(2) break;
+                default: GRG_LEAN_WARP(3) break;
             }
 #undef GRG_LEAN_WARP
             GRG_LAUNCH_CHECK("level_lean_warp_kernel");
@@ -2815,9 +2601,7 @@ int build_level_args(const grg_b200_traverse_args* a, const Shape& sh, const grg
     return GRG_B200_OK;
 }
 
-int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level* L, const void* blob, cudaStream_t s,
-              const ChainInfo& ci = ChainInfo{}, bool* chained = nullptr) {
-    if (chained) *chained = false;
+int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_level* L, const void* blob, cudaStream_t s) {
     if (L->num_rows < 0 || L->num_heavy < 0 || L->num_entries < 0)
         return fail(GRG_B200_ERR_INVALID, "negative level sizes");
     if (L->num_rows == 0) return GRG_B200_OK;
@@ -2828,8 +2612,7 @@ int run_level(const grg_b200_traverse_args* a, const Shape& sh, const grg_b200_l
     if (a->dtype == GRG_B200_MIXED) return launch_level_mx(la, a->init_mode, a->narrow_variant, s);
     return dispatch(a, sh, [&](auto t, auto v) {
         return launch_level_typed<decltype(t), decltype(v)::value>(la, a->init_mode, exact, a->narrow_variant, a->heavy_variant,
-                                                                   a->persist_ctas, (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0, s,
-                                                                   ci, chained);
+                                                                   a->persist_ctas, (a->launch_flags & GRG_B200_LAUNCH_PDL) != 0, s);
     });
 }
 
@@ -3399,11 +3182,6 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
         GRG_CUDA_TRY(cudaEventRecord(a->ring->fork, s));
         GRG_CUDA_TRY(cudaStreamWaitEvent(a->ring->copy, a->ring->fork, 0));
     }
-    // Chained traversal: each level launch triggers the next only after its wait, so a launch
-    // may add the sources written two or more launches back before its own wait.
-    const bool chain_mode = (a->launch_flags & GRG_B200_LAUNCH_EARLY) && (a->launch_flags & GRG_B200_LAUNCH_PDL) && !any_streamed &&
-                            a->fuse_entries <= 0;
-    ChainInfo ci;
     for (int i = 0; i < a->num_levels; ++i) {
         if (a->fuse_entries > 0) {  // a run of small resident levels: one cooperative launch
             static thread_local LevelArgs run_las[kRunMaxLevels];
@@ -3434,15 +3212,8 @@ int grg_b200_traverse(const grg_b200_traverse_args* a, void* stream_handle) {
             GRG_CUDA_TRY(cudaStreamWaitEvent(s, r->ready[L.ring_slot], 0));
             blob = a->slot_buffers[L.ring_slot];
         }
-        bool chained = false;
-        ci.chain = chain_mode;
-        rc = run_level(a, sh, &L, blob, s, ci, &chained);
+        rc = run_level(a, sh, &L, blob, s);
         if (rc) return rc;
-        if (L.num_rows > 0) {  // the next launch's late rows are this level's
-            ci.early = chained;
-            ci.late_lo = static_cast<uint32_t>(L.row_begin);
-            ci.late_n = static_cast<uint32_t>(L.num_rows);
-        }
         if (L.ring_slot >= 0 && L.num_rows > 0) {
             GRG_CUDA_TRY(cudaEventRecord(a->ring->free_ev[L.ring_slot], s));
             used[L.ring_slot] = true;

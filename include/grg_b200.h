@@ -233,11 +233,8 @@ typedef struct grg_b200_traverse_args {
                                            warp per row (lane groups split the list, shuffle
                                            reduction); 2 as 1 but in the same launch as the narrow
                                            rows (narrow_variant 6 to 10 only; otherwise as 1); 3 as 1
-                                           with 32 heavy rows (1024 threads) per CTA; 4 as 2
-                                           with narrow_variant 13 / 14's entry-parallel walk
-                                           for the heavy rows too (a warp of W chunk lanes x
-                                           32 / W entry slots, 32-byte loads; otherwise as 2).
-                                           Exact order always uses one CTA per row. */
+                                           with 32 heavy rows (1024 threads) per CTA.  Exact
+                                           order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of
                                            num_mutations rows and ld_state columns */
@@ -266,14 +263,6 @@ typedef struct grg_b200_traverse_args {
  * level lists until the hardware reports that kernel complete, and so overlaps the launch
  * gap.  Ignored when any level is streamed. */
 #define GRG_B200_LAUNCH_PDL 1
-/* With GRG_B200_LAUNCH_PDL and resident levels: chain the level launches.  Each level kernel
- * lets the next launch start only after its own wait on the previous one, so while launch i
- * runs, launches up to i - 2 are complete; from the second level launch on, the narrow
- * variant 14 walks (and the heavy walk of all-heavy levels) add every source that the
- * previous launch does not write before their wait, and only the rest after it.  Lists hold
- * a row's sources by level, the previous launch's last, as the list builders write them.
- * Other kernels run unchained. */
-#define GRG_B200_LAUNCH_EARLY 2
 
 /*
  * GRG_B200_SCHEDULE_LEVELS: one launch per level (each level waits for the previous one).

@@ -130,42 +130,15 @@ def test_golden_mixed_precision(group, heavy, golden_data):
         assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("threshold", [4, 128])
-@pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
-def test_golden_early_sources(group, threshold, golden_data):
-    """Chained level launches (``early_sources``, sources older than the previous launch added
-    before each wait) on every golden case: exact for integer-valued inputs, within tolerance
-    otherwise; with and without heavy rows."""
-    from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
-
-    name, dtype = group
-    plan = B200Plan(heavy_threshold=threshold, narrow_split=0, early_sources=True)
-    layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), pair=B200PlanPair(plan_up=plan, plan_down=plan))
-    rtol, atol = (RTOL_F64, ATOL_F64) if dtype == "float64" else (RTOL_F32, ATOL_F32)
-    with B200Runtime(layout, check_bounds=False) as runtime:
-        (grg,) = runtime.grgs
-        for case in GROUPS[group]:
-            out, miss = _run_case(grg, case, golden_data)
-            expected = golden_data[case["key"] + "|out"]
-            integer = any(tag in case["case"] for tag in ("pm1", "ones", "zeros"))
-            if integer and case["init"] is None:
-                np.testing.assert_array_equal(out, expected, err_msg=case["key"])
-            else:
-                np.testing.assert_allclose(out, expected, rtol=rtol, atol=atol * max(1.0, np.abs(expected).max()), err_msg=case["key"])
-        assert runtime.device_error() == 0
-
-
-@pytest.mark.parametrize("heavy", [2, 4])
 @pytest.mark.parametrize("variant", [13, 14])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
-def test_golden_entry_walks_with_heavy_rows(group, variant, heavy, golden_data):
-    """The entry-parallel walks with many heavy rows (threshold 4), walked either 16 bytes at a
-    time in quads (heavy_variant 2) or entry-parallel in 32-byte chunks (heavy_variant 4):
-    exact for integer-valued inputs, within tolerance otherwise."""
+def test_golden_entry_walks_with_heavy_rows(group, variant, golden_data):
+    """The entry-parallel walks with many heavy rows (threshold 4) in the same launch, and the
+    short one-slot rows: exact for integer-valued inputs, within tolerance otherwise."""
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
 
     name, dtype = group
-    plan = B200Plan(narrow_variant=variant, heavy_variant=heavy, heavy_threshold=4, narrow_split=0)
+    plan = B200Plan(narrow_variant=variant, heavy_variant=2, heavy_threshold=4, narrow_split=0)
     layout = _layout([artifact_path(name)], dtype=np.dtype(dtype), pair=B200PlanPair(plan_up=plan, plan_down=plan))
     rtol, atol = (RTOL_F64, ATOL_F64) if dtype == "float64" else (RTOL_F32, ATOL_F32)
     with B200Runtime(layout, check_bounds=False) as runtime:

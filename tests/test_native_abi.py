@@ -43,7 +43,6 @@ def test_header_constants_match_binding():
     assert define("GRG_B200_NARROW_VARIANTS") == nat.NARROW_VARIANTS
     assert define("GRG_B200_MAX_SLOT_BUCKETS") == nat.MAX_SLOT_BUCKETS
     assert define("GRG_B200_LAUNCH_PDL") == nat.LAUNCH_PDL
-    assert define("GRG_B200_LAUNCH_EARLY") == nat.LAUNCH_EARLY
     assert define("GRG_B200_DEVICE_WAIT_TIMEOUT") == nat.DEVICE_WAIT_TIMEOUT
 
 
