@@ -873,23 +873,32 @@ __device__ __forceinline__ typename Chunk32<T>::type ld_chunk(const T* p) {
     return r;
 }
 
+// One chunk lane's CW columns: a 32-byte load when CW fills a chunk, else the shape's vector
+// load (k below a chunk: CW = k, one chunk lane per row).
+template <typename T, int CW>
+__device__ __forceinline__ Pack<T, CW> ld_cols(const T* p) {
+    if constexpr (CW == Chunk32<T>::C) return ld_chunk<T>(p);
+    else return ld_ro<T, CW>(p);
+}
+
 // Narrow rows, entry-parallel (narrow_variant 13, default mode only).  A row's lane group of G
 // lanes is W chunk lanes x 2 entry slots (W = k / C, C columns per 32-byte chunk): lane (e, w)
 // adds chunk w of entries e and e + 2 of every 4-entry quad, so each code is decoded by W lanes
 // instead of G and a row fetch is one 32-byte load per chunk.  The two slots' sums are added by
 // one shuffle and the slot-0 lanes store.  The order of additions differs from the reference's
 // (exact for integer-valued inputs, reassociation otherwise).  log2w = log2(W), G = 2W.
-template <typename T, int INIT, bool UPONLY>
+template <typename T, int INIT, bool UPONLY, int CW>
 __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
-    using Ch = typename Chunk32<T>::type;
-    constexpr int C = Chunk32<T>::C;
+    using Ch = Pack<T, CW>;
+    constexpr int C = CW;  // columns per chunk lane
+    const int lg = a.log2g + (CW == Chunk32<T>::C ? 0 : 1);  // log2 of the 2W lanes of a row
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy - a.short_rows;  // the short rows follow
-    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - lg)) + (lane >> lg);
     const bool live = pos < narrow;  // dead lanes still join the shuffle
-    const int glane = lane & ((1 << a.log2g) - 1);
-    const int log2w = a.log2g - 1;
+    const int glane = lane & ((1 << lg) - 1);
+    const int log2w = lg - 1;
     const int w = glane & ((1 << log2w) - 1);
     const int e = glane >> log2w;  // entry slot 0 or 1
     int32_t q0 = 0, q1 = 0;
@@ -914,8 +923,8 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
         bool ok0, ok1;
         const T* p0 = lean_source<T, UPONLY>(a, c0, ok0);
         const T* p1 = lean_source<T, UPONLY>(a, c1, ok1);
-        const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-        const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+        const Ch v0 = ok0 ? ld_cols<T, CW>(p0 + c) : zero_pack<T, C>();
+        const Ch v1 = ok1 ? ld_cols<T, CW>(p1 + c) : zero_pack<T, C>();
         add_into(acc, v0);
         add_into(acc, v1);
         cur = nxt;
@@ -936,17 +945,18 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
 // rest one round ahead, as entry_rows does.
 constexpr int kPreQuads = 4;
 
-template <typename T, int INIT, bool UPONLY>
+template <typename T, int INIT, bool UPONLY, int CW>
 __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block) {
-    using Ch = typename Chunk32<T>::type;
-    constexpr int C = Chunk32<T>::C;
+    using Ch = Pack<T, CW>;
+    constexpr int C = CW;  // columns per chunk lane
+    const int lg = a.log2g + (CW == Chunk32<T>::C ? 0 : 1);  // log2 of the 2W lanes of a row
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy - a.short_rows;  // the short rows follow
-    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - lg)) + (lane >> lg);
     const bool live = pos < narrow;  // dead lanes still join the shuffle
-    const int glane = lane & ((1 << a.log2g) - 1);
-    const int log2w = a.log2g - 1;
+    const int glane = lane & ((1 << lg) - 1);
+    const int log2w = lg - 1;
     const int w = glane & ((1 << log2w) - 1);
     const int e = glane >> log2w;  // entry slot 0 or 1
     int32_t q0 = 0, q1 = 0;
@@ -978,8 +988,8 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
             bool ok0, ok1;
             const T* p0 = lean_source<T, UPONLY>(a, pre0[j], ok0);
             const T* p1 = lean_source<T, UPONLY>(a, pre1[j], ok1);
-            const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-            const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+            const Ch v0 = ok0 ? ld_cols<T, CW>(p0 + c) : zero_pack<T, C>();
+            const Ch v1 = ok1 ? ld_cols<T, CW>(p1 + c) : zero_pack<T, C>();
             add_into(acc, v0);
             add_into(acc, v1);
         }
@@ -994,8 +1004,8 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
             bool ok0, ok1;
             const T* p0 = lean_source<T, UPONLY>(a, c0, ok0);
             const T* p1 = lean_source<T, UPONLY>(a, c1, ok1);
-            const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-            const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+            const Ch v0 = ok0 ? ld_cols<T, CW>(p0 + c) : zero_pack<T, C>();
+            const Ch v1 = ok1 ? ld_cols<T, CW>(p1 + c) : zero_pack<T, C>();
             add_into(acc, v0);
             add_into(acc, v1);
             cur = nxt;
@@ -1015,13 +1025,14 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
 // 32-byte chunk of all the row's entries, left to right, so a warp covers 32 / W rows, twice as
 // many as entry_rows, and a level of short rows needs half the CTAs.  The codes load before the
 // wait; a longer list is still summed in full (one quad ahead, as entry_rows).
-template <typename T, int INIT, bool UPONLY>
+template <typename T, int INIT, bool UPONLY, int CW>
 __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t block) {
-    using Ch = typename Chunk32<T>::type;
-    constexpr int C = Chunk32<T>::C;
+    using Ch = Pack<T, CW>;
+    constexpr int C = CW;  // columns per chunk lane
+    const int lg = a.log2g + (CW == Chunk32<T>::C ? 0 : 1);  // log2 of the 2W lanes of a row
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int log2w = a.log2g - 1;
+    const int log2w = lg - 1;
     const int64_t narrow = a.num_rows - a.num_heavy;
     const int64_t pos = narrow - a.short_rows + ((block * kNarrowWarps + warp) << (5 - log2w)) + (lane >> log2w);
     const bool live = pos < narrow;
@@ -1050,8 +1061,8 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
             bool ok0, ok1;
             const T* p0 = lean_source<T, UPONLY>(a, code[u], ok0);
             const T* p1 = lean_source<T, UPONLY>(a, code[u + 1], ok1);
-            const Ch v0 = ok0 ? ld_chunk<T>(p0 + c) : zero_pack<T, C>();
-            const Ch v1 = ok1 ? ld_chunk<T>(p1 + c) : zero_pack<T, C>();
+            const Ch v0 = ok0 ? ld_cols<T, CW>(p0 + c) : zero_pack<T, C>();
+            const Ch v1 = ok1 ? ld_cols<T, CW>(p1 + c) : zero_pack<T, C>();
             add_into(acc, v0);
             add_into(acc, v1);
         }
@@ -1064,23 +1075,23 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
 
 // narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (lean walk), the next
 // long_blocks the two-slot narrow rows, the rest the short rows.
-template <typename T, int INIT, bool UPONLY>
+template <typename T, int INIT, bool UPONLY, int CW>
 __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
     const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
-    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY>(a, b - heavy_blocks);
-    else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
+    if (b < heavy_blocks) lean_heavy_rows<T, (CW == Chunk32<T>::C ? CW / 2 : CW), INIT, UPONLY>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY, CW>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY, CW>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 13: as 14 with entry_rows for the two-slot narrow rows.
-template <typename T, int INIT, bool UPONLY>
+template <typename T, int INIT, bool UPONLY, int CW>
 __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
     const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) lean_heavy_rows<T, Chunk32<T>::C / 2, INIT, UPONLY>(a, b);
-    else if (b < heavy_blocks + long_blocks) entry_rows<T, INIT, UPONLY>(a, b - heavy_blocks);
-    else entry_short_rows<T, INIT, UPONLY>(a, b - heavy_blocks - long_blocks);
+    if (b < heavy_blocks) lean_heavy_rows<T, (CW == Chunk32<T>::C ? CW / 2 : CW), INIT, UPONLY>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows<T, INIT, UPONLY, CW>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY, CW>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
@@ -2298,26 +2309,32 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
     if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
-        const bool shape = lean && V == C / 2 && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE && la.log2g >= 1 &&
-                           (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 && la.ld_x % C == 0 &&
-                           (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
-                           (!la.use_miss || aligned(la.miss, 32));
-        if (shape) {
+        const bool common = lean && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE;
+        // 32-byte chunks: k = 2^n chunks of C columns (the shape's V = C / 2 columns per lane)
+        const bool chunks = common && V == C / 2 && la.log2g >= 1 && (int64_t{V} << la.log2g) == la.k && la.ld_state % C == 0 &&
+                            la.ld_x % C == 0 && (!la.use_miss || la.ld_miss % C == 0) && aligned(la.state, 32) && aligned(la.x, 32) &&
+                            (!la.use_miss || aligned(la.miss, 32));
+        // k below a chunk: one chunk lane of the shape's V = k columns (the shape's alignment)
+        const bool narrow_k = common && !chunks && V < C && la.log2g == 0 && la.k == V;
+        if (chunks || narrow_k) {
             constexpr int rows_per_cta = kWarpRowThreads / 32;
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
-            const int log2w = la.log2g - 1;  // one entry slot: W = G / 2 lanes per short row
+            const int lg = la.log2g + (chunks ? 0 : 1);  // log2 of a row's 2W lanes
+            const int log2w = lg - 1;                    // one entry slot: W lanes per short row
             const int64_t long_rows = narrow - la.short_rows;
-            const int64_t long_warps = (long_rows + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+            const int64_t long_warps = (long_rows + (32 >> lg) - 1) >> (5 - lg);
             const int64_t short_warps = (la.short_rows + (32 >> log2w) - 1) >> (5 - log2w);
             const int64_t long_blocks = (long_warps + kNarrowWarps - 1) / kNarrowWarps;
             const dim3 grid(static_cast<unsigned>(heavy_blocks + long_blocks + (short_warps + kNarrowWarps - 1) / kNarrowWarps));
+#define GRG_ENTRY(KERNEL, CW)                                                                                                   \
+    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, true, CW>, la, heavy_blocks, long_blocks)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, false, CW>, la, heavy_blocks, long_blocks));
             if (variant == 13) {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
+                if (chunks) { GRG_ENTRY(level_entry_kernel, C) } else { GRG_ENTRY(level_entry_kernel, V) }
             } else {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, true>, la, heavy_blocks, long_blocks));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, level_entry_pre_kernel<T, 0, false>, la, heavy_blocks, long_blocks));
+                if (chunks) { GRG_ENTRY(level_entry_pre_kernel, C) } else { GRG_ENTRY(level_entry_pre_kernel, V) }
             }
+#undef GRG_ENTRY
             GRG_LAUNCH_CHECK("level_entry_kernel");
             return GRG_B200_OK;
         }

@@ -652,12 +652,13 @@ def test_short_row_walk_sums_any_list_length(synth_artifact, variant, k):
             assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("k", [1, 3, 8, 16, 33])
+@pytest.mark.parametrize("k", [1, 2, 3, 8, 16, 33])
 def test_lean_walks_match_variant_7_and_the_oracle(synth_artifact, k):
-    """Narrow variants 11, 12 and 13 (the lean walks, used by launches without a bounds-check
-    word and without row splits) on every mode of the hot path: 11 returns the same bits as 7;
-    12 (one partial sum per row) and 13 (entry-parallel rows, where k and the init allow it)
-    are exact for integer-valued inputs and within 1e-12 otherwise."""
+    """Narrow variants 11 to 14 (the lean walks, used by launches without a bounds-check word
+    and without row splits) on every mode of the hot path: 11 returns the same bits as 7 and 14
+    the same as 13; 12 (one partial sum per row) and 13 (entry-parallel rows, in 32-byte
+    chunks, or one vector per lane at k = 1 and 2, where the init allows it) are exact for
+    integer-valued inputs and within 1e-12 otherwise."""
     from grg_spmv_b200.backends.b200 import B200Plan, B200PlanPair, B200Runtime
 
     oracle = OracleGRG(synth_artifact)
