@@ -223,6 +223,8 @@ typedef struct grg_b200_traverse_args {
                                            vector width, no init, 32-byte aligned buffers;
                                            otherwise as 12); 14: as 13 with the codes of a row's
                                            first 4 quads loaded before the previous level ends.
+                                           At k = V (k below a 32-byte chunk: k = 1, 2 in FP64)
+                                           13 and 14 walk one V-column chunk lane per row.
                                            13 and 14 walk a level's short_rows with one entry
                                            slot (each lane adds its chunk of all 4 entries).
                                            11 to 14 fall back to 7 with an
