@@ -62,10 +62,11 @@ class B200Plan:
     ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
     processed together); None picks the direction's default (up natural, down locality).
     ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``); None
-    picks per call, as measured on B200: in the default mode the lean walks 14 for k <= 2 and
-    8 <= k <= 16 and 13 above (both run as 12 where their shape does not apply), 12 for
-    3 <= k < 8; in exact order 7 for k <= 16 and 6 above; with ``pad_lists=False``, 5.
-    Runtimes with bounds checking run 7 in place of 11-14.
+    picks per call, as measured on B200: in the default mode the lean entry-parallel walk 14
+    (run as 12 where its shape does not apply: k not a power of two, or above 64 in FP64 and
+    128 in FP32); in exact
+    order 7 for k <= 16 and 6 above; with ``pad_lists=False``, 5.  Runtimes with bounds
+    checking run 7 in place of 11-14.
     ``balance``: group narrow rows by length (power-of-two buckets) so a warp's rows finish
     together.
     ``autotune``: time the narrow-kernel variants, then the heavy-row kernels, when the runtime
@@ -153,14 +154,10 @@ class B200Plan:
         # the lean walks, measured on B200 (config 2): one partial sum per row (12) +17% over 7
         # at k = 8 and +14% over 6 at k = 32; entry-parallel rows (13, else as 12) a further +2%
         # at k = 8 and +3% at k = 16 and 32, but -2% at k = 4; their codes loaded before the
-        # previous level ends (14) +2.5% at k = 8, +1% at k = 16, -1.5% at k = 32; below a
-        # 32-byte chunk, one vector per lane (14 at k = 1 and 2) +9.5% over 7 at k = 1 and +8.4%
-        # over 12 at k = 2
-        if int(k) <= 2 or 8 <= int(k) <= 16:
-            return 14
-        if int(k) > 16:
-            return 13
-        return 12
+        # previous level ends (14) +2.5% at k = 8 and +1% at k = 16 over 13; with one-slot short
+        # rows, 14 over 13 +0.6% at k = 32 and over 12 +1.1% at k = 4; below a 32-byte chunk,
+        # one vector per lane, +9.5% over 7 at k = 1 and +8.4% over 12 at k = 2
+        return 14
 
     def resolve_pdl(self, k: int) -> bool:
         """Whether calls with ``k`` right-hand sides use programmatic dependent launch."""
