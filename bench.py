@@ -14,20 +14,22 @@ ops' shared ``io0`` buffer).  Metric: edge·RHS/s = steps · 2·E·k / device ti
   pinned host memory and both outputs copied back every step; ``--e2e-inflight`` steps (8)
   run at once, each on its own runtime and stream, so one step's copies overlap another's
   kernels (the host link moves 70 MB each way per step at about 95 GB/s in both directions
-  together, 1.5 ms, against 1.45 ms of kernels).
+  together, 1.5 ms, against 1.4 ms of kernels).
 * ``roofline``: the level gather kernels timed live in one instrumented up+down pass: events
   around each direction's level launches, issued back to back as in the recorded graph (a
   second pass with events around every launch prints the per-level breakdown to stderr).  Algorithmic bytes per level: 4 per gather entry and row
   pointer, plus each destination row written once and read once later (2·k·8); plus, for
   down, the mutation and miss input rows read once.  ``traffic`` is the DRAM traffic (read +
   write) of one up-level-1 launch measured by ncu on the same configuration;
-  ``traffic_launches`` lists it with down levels 3 and 0, beside this run's own timing and
-  algorithmic bytes of those launches.
+  ``traffic_launches`` lists it with down levels 3, 1 and 0, beside this run's own timing
+  and algorithmic bytes of those launches.
 * ``cpu_baseline``: the oracle (SciPy restatement of the reference's ReferenceRuntime) on one
   step of the same graph, RHS columns split over one process per host core (up to k), rank 0,
   N=1 only.
 * ``tiers``: RHS-block batching and mixed precision against the plain FP64 drop-in on the same
-  graph and on eight generated graphs (N=1 only; ``--no-tiers`` skips it).
+  graph and on eight generated graphs, the standardised Gram operator, and the precision
+  configuration (diploid config-2 graph, k = 32, init_xtx, plain and mixed node state against
+  the oracle) (N=1 only; ``--no-tiers`` skips it).
 * ``--impl reference``: the reference's CPU path (the oracle port; the pure-Python reference
   cannot be installed offline) timed on the same workload, on the same host cores.
 
@@ -45,6 +47,7 @@ import os
 from pathlib import Path
 import subprocess
 import sys
+import shutil
 import tempfile
 import time
 
@@ -653,6 +656,21 @@ def run_b200(args) -> None:
         tiers = {"single_graph": measure_tiers(args, [path], device, stream, [config_blocks])[0]}
         torch.cuda.empty_cache()
         tiers["pca_operator"] = measure_xtx_operator(path, device)
+        torch.cuda.empty_cache()
+
+        def timed(st, fn):  # events on the stream, host clock beside them
+            torch.cuda.synchronize(device)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            t0 = time.perf_counter()
+            a.record(st)
+            res = fn()
+            b.record(st)
+            torch.cuda.synchronize(device)
+            return res, a.elapsed_time(b), (time.perf_counter() - t0) * 1e3
+
+        # the precision configuration (diploid config-2 graph, k = 32, init_xtx; plain and mixed)
+        tiers["precision"] = run_precision(args, timed, device)
+        torch.cuda.empty_cache()
         if args.tier_grgs > 0:
             t0 = time.perf_counter()
             multi = make_multi_artifacts(args)
@@ -1085,7 +1103,8 @@ def run_precision(args, timed, device) -> dict:
     from grg_spmv_b200.backends.b200 import B200Runtime, plan_b200_layout
     from grg_spmv_b200.synth import CONFIG2, write_synthetic_artifact
 
-    path = Path(args.precision_artifact) if args.precision_artifact else Path(tempfile.mkdtemp(prefix="grg_prec_")) / "config2_diploid.grg_spmv"
+    tmpdir = None if args.precision_artifact else Path(tempfile.mkdtemp(prefix="grg_prec_"))
+    path = Path(args.precision_artifact) if args.precision_artifact else tmpdir / "config2_diploid.grg_spmv"
     gen_s = 0.0
     if not path.exists():
         t0 = time.perf_counter()
@@ -1145,6 +1164,8 @@ def run_precision(args, timed, device) -> dict:
         m_up, m_dn = results[("mixed", name)]
         p_up, p_dn = results[("plain", name)]
         out["mixed"][f"max_rel_err_vs_plain_f64_{name}"] = max(rel(m_up, p_up), rel(m_dn, p_dn))
+    if tmpdir is not None:  # the generated graph is this call's own
+        shutil.rmtree(tmpdir, ignore_errors=True)
     return out
 
 
