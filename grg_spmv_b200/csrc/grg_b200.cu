@@ -882,11 +882,12 @@ __device__ __forceinline__ Pack<T, CW> ld_cols(const T* p) {
 }
 
 // Narrow rows, entry-parallel (narrow_variant 13, default mode only).  A row's lane group of G
-// lanes is W chunk lanes x 2 entry slots (W = k / C, C columns per 32-byte chunk): lane (e, w)
-// adds chunk w of entries e and e + 2 of every 4-entry quad, so each code is decoded by W lanes
-// instead of G and a row fetch is one 32-byte load per chunk.  The two slots' sums are added by
-// one shuffle and the slot-0 lanes store.  The order of additions differs from the reference's
-// (exact for integer-valued inputs, reassociation otherwise).  log2w = log2(W), G = 2W.
+// lanes is W chunk lanes x 2 entry slots (W = k / CW): lane (e, w) adds chunk w of entries e and
+// e + 2 of every 4-entry quad, so each code is decoded by W lanes instead of G and a row fetch
+// is one load per chunk.  CW is a 32-byte chunk's columns, or, when k is a single vector of the
+// shape (k below a chunk), k itself (W = 1).  The two slots' sums are added by one shuffle and
+// the slot-0 lanes store.  The order of additions differs from the reference's (exact for
+// integer-valued inputs, reassociation otherwise).  log2w = log2(W), G = 2W = 2^lg.
 template <typename T, int INIT, bool UPONLY, int CW>
 __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
     using Ch = Pack<T, CW>;
