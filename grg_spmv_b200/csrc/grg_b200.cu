@@ -888,7 +888,7 @@ __device__ __forceinline__ Pack<T, CW> ld_cols(const T* p) {
 // shape (k below a chunk), k itself (W = 1).  The two slots' sums are added by one shuffle and
 // the slot-0 lanes store.  The order of additions differs from the reference's (exact for
 // integer-valued inputs, reassociation otherwise).  log2w = log2(W), G = 2W = 2^lg.
-template <typename T, int INIT, bool UPONLY, int CW>
+template <typename T, int INIT, bool UPONLY, int CW, int NW = kNarrowWarps>
 __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
     using Ch = Pack<T, CW>;
     constexpr int C = CW;  // columns per chunk lane
@@ -896,7 +896,7 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy - a.short_rows;  // the short rows follow
-    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - lg)) + (lane >> lg);
+    const int64_t pos = ((block * NW + warp) << (5 - lg)) + (lane >> lg);
     const bool live = pos < narrow;  // dead lanes still join the shuffle
     const int glane = lane & ((1 << lg) - 1);
     const int log2w = lg - 1;
@@ -946,7 +946,7 @@ __device__ __forceinline__ void entry_rows(const LevelArgs& a, int64_t block) {
 // rest one round ahead, as entry_rows does.
 constexpr int kPreQuads = 4;
 
-template <typename T, int INIT, bool UPONLY, int CW>
+template <typename T, int INIT, bool UPONLY, int CW, int NW = kNarrowWarps>
 __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block) {
     using Ch = Pack<T, CW>;
     constexpr int C = CW;  // columns per chunk lane
@@ -954,7 +954,7 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy - a.short_rows;  // the short rows follow
-    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - lg)) + (lane >> lg);
+    const int64_t pos = ((block * NW + warp) << (5 - lg)) + (lane >> lg);
     const bool live = pos < narrow;  // dead lanes still join the shuffle
     const int glane = lane & ((1 << lg) - 1);
     const int log2w = lg - 1;
@@ -1026,7 +1026,7 @@ __device__ __forceinline__ void entry_rows_pre(const LevelArgs& a, int64_t block
 // 32-byte chunk of all the row's entries, left to right, so a warp covers 32 / W rows, twice as
 // many as entry_rows, and a level of short rows needs half the CTAs.  The codes load before the
 // wait; a longer list is still summed in full (one quad ahead, as entry_rows).
-template <typename T, int INIT, bool UPONLY, int CW>
+template <typename T, int INIT, bool UPONLY, int CW, int NW = kNarrowWarps>
 __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t block) {
     using Ch = Pack<T, CW>;
     constexpr int C = CW;  // columns per chunk lane
@@ -1035,7 +1035,7 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
     const int lane = threadIdx.x & 31;
     const int log2w = lg - 1;
     const int64_t narrow = a.num_rows - a.num_heavy;
-    const int64_t pos = narrow - a.short_rows + ((block * kNarrowWarps + warp) << (5 - log2w)) + (lane >> log2w);
+    const int64_t pos = narrow - a.short_rows + ((block * NW + warp) << (5 - log2w)) + (lane >> log2w);
     const bool live = pos < narrow;
     const int w = lane & ((1 << log2w) - 1);
     int32_t q0 = 0, q1 = 0;
@@ -1076,13 +1076,15 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
 
 // narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (lean walk), the next
 // long_blocks the two-slot narrow rows, the rest the short rows.
-template <typename T, int INIT, bool UPONLY, int CW>
-__global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
+// NW warps per CTA: 8 (narrow_variant 14), or 4 (15: finer-grained CTAs at the same 40 warps
+// per SM).
+template <typename T, int INIT, bool UPONLY, int CW, int NW = kNarrowWarps>
+__global__ void __launch_bounds__(32 * NW, 40 / NW) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
     const int64_t b = blockIdx.x;
-    if (b < heavy_blocks) lean_heavy_rows<T, (CW == Chunk32<T>::C ? CW / 2 : CW), INIT, UPONLY>(a, b);
-    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY, CW>(a, b - heavy_blocks);
-    else entry_short_rows<T, INIT, UPONLY, CW>(a, b - heavy_blocks - long_blocks);
+    if (b < heavy_blocks) lean_heavy_rows<T, (CW == Chunk32<T>::C ? CW / 2 : CW), INIT, UPONLY, NW>(a, b);
+    else if (b < heavy_blocks + long_blocks) entry_rows_pre<T, INIT, UPONLY, CW, NW>(a, b - heavy_blocks);
+    else entry_short_rows<T, INIT, UPONLY, CW, NW>(a, b - heavy_blocks - long_blocks);
 }
 
 // narrow_variant 13: as 14 with entry_rows for the two-slot narrow rows.
@@ -2308,7 +2310,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
-    if (variant == 13 || variant == 14) {  // entry-parallel narrow rows where the shape allows it, else as 12
+    if (variant == 13 || variant == 14 || variant == 15) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
         const bool common = lean && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE;
         // 32-byte chunks: k = 2^n chunks of C columns (the shape's V = C / 2 columns per lane)
@@ -2318,22 +2320,28 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         // k below a chunk: one chunk lane of the shape's V = k columns (the shape's alignment)
         const bool narrow_k = common && !chunks && V < C && la.log2g == 0 && la.k == V;
         if (chunks || narrow_k) {
-            constexpr int rows_per_cta = kWarpRowThreads / 32;
-            const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
+            const int nw = variant == 15 ? 4 : kNarrowWarps;  // warps per CTA; heavy rows: one each
+            const int64_t heavy_blocks = (la.num_heavy + nw - 1) / nw;
             const int lg = la.log2g + (chunks ? 0 : 1);  // log2 of a row's 2W lanes
             const int log2w = lg - 1;                    // one entry slot: W lanes per short row
             const int64_t long_rows = narrow - la.short_rows;
             const int64_t long_warps = (long_rows + (32 >> lg) - 1) >> (5 - lg);
             const int64_t short_warps = (la.short_rows + (32 >> log2w) - 1) >> (5 - log2w);
-            const int64_t long_blocks = (long_warps + kNarrowWarps - 1) / kNarrowWarps;
-            const dim3 grid(static_cast<unsigned>(heavy_blocks + long_blocks + (short_warps + kNarrowWarps - 1) / kNarrowWarps));
+            const int64_t long_blocks = (long_warps + nw - 1) / nw;
+            const dim3 grid(static_cast<unsigned>(heavy_blocks + long_blocks + (short_warps + nw - 1) / nw));
 #define GRG_ENTRY(KERNEL, CW)                                                                                                   \
     if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, true, CW>, la, heavy_blocks, long_blocks)); \
     else GRG_CUDA_TRY(launch_k(pdl, s, grid, kNarrowThreads, KERNEL<T, 0, false, CW>, la, heavy_blocks, long_blocks));
             if (variant == 13) {
                 if (chunks) { GRG_ENTRY(level_entry_kernel, C) } else { GRG_ENTRY(level_entry_kernel, V) }
-            } else {
+            } else if (variant == 14) {
                 if (chunks) { GRG_ENTRY(level_entry_pre_kernel, C) } else { GRG_ENTRY(level_entry_pre_kernel, V) }
+            } else {
+#define GRG_ENTRY4(CW)                                                                                                        \
+    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_entry_pre_kernel<T, 0, true, CW, 4>, la, heavy_blocks, long_blocks)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_entry_pre_kernel<T, 0, false, CW, 4>, la, heavy_blocks, long_blocks));
+                if (chunks) { GRG_ENTRY4(C) } else { GRG_ENTRY4(V) }
+#undef GRG_ENTRY4
             }
 #undef GRG_ENTRY
             GRG_LAUNCH_CHECK("level_entry_kernel");
