@@ -244,6 +244,7 @@ CONFIG2_K8_TRAFFIC = {
     ("down", 1): {"kernel": "level_entry_pre_kernel", "dram_bytes": 524657152 + 21673984, "ncu_us": 115.74},
     ("down", 0): {"kernel": "level_lean_warp_kernel", "dram_bytes": 457806336 + 16741120, "ncu_us": 208.93},
 }
+CONFIG2_K8_VARIANT = 14  # the narrow variant those launches ran
 TRAFFIC_SOURCE = "profiles/level_traffic_config2_k8.md (ncu -c 1 per launch on the config-2 graph, k = 8)"
 
 
@@ -685,7 +686,8 @@ def run_b200(args) -> None:
     # launch of the same configuration.
     traffic, traffic_launches = None, None
     captured = (args.workload == "config2" and k == 8 and args.precision == "plain" and pair.plan_down.schedule == "levels"
-                and not args.heavy_buckets and not args.no_short_rows and narrow_used == {"up": 14, "down": 14} and launch_ms)
+                and not args.heavy_buckets and not args.no_short_rows and launch_ms
+                and narrow_used == {"up": CONFIG2_K8_VARIANT, "down": CONFIG2_K8_VARIANT})
     if captured:
         traffic_launches = []
         for (direction, level), cap in CONFIG2_K8_TRAFFIC.items():

@@ -57,7 +57,7 @@ SRC_SHIFT = 29
 SRC_STATE, SRC_INPUT, SRC_MISS, SRC_NULL = 0, 1, 2, 3
 ID_MASK = 0x1FFFFFFF
 MAX_ID = 0x1FFFFFFF
-NARROW_VARIANTS = 16
+NARROW_VARIANTS = 17
 
 
 class Level(ctypes.Structure):

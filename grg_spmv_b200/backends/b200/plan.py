@@ -62,8 +62,8 @@ class B200Plan:
     ``row_order``: "natural" (node order) or "locality" (rows that share source rows are
     processed together); None picks the direction's default (up natural, down locality).
     ``narrow_variant``: shape of the narrow-row kernel (``GRG_B200_NARROW_VARIANTS``); None
-    picks per call, as measured on B200: in the default mode the lean entry-parallel walk 14
-    (run as 12 where its shape does not apply: k not a power of two, or above 64 in FP64 and
+    picks per call, as measured on B200: in the default mode the lean entry-parallel walk in
+    4-warp CTAs, 15 (run as 12 where its shape does not apply: k not a power of two, or above 64 in FP64 and
     128 in FP32); in exact
     order 7 for k <= 16 and 6 above; with ``pad_lists=False``, 5.  Runtimes with bounds
     checking run 7 in place of 11-14.
@@ -156,8 +156,9 @@ class B200Plan:
         # at k = 8 and +3% at k = 16 and 32, but -2% at k = 4; their codes loaded before the
         # previous level ends (14) +2.5% at k = 8 and +1% at k = 16 over 13; with one-slot short
         # rows, 14 over 13 +0.6% at k = 32 and over 12 +1.1% at k = 4; below a 32-byte chunk,
-        # one vector per lane, +9.5% over 7 at k = 1 and +8.4% over 12 at k = 2
-        return 14
+        # one vector per lane, +9.5% over 7 at k = 1 and +8.4% over 12 at k = 2; the same walk
+        # in 4-warp CTAs (15) a further +1.9% at k = 8, +2.7% at k = 32, +0.9% at k = 1
+        return 15
 
     def resolve_pdl(self, k: int) -> bool:
         """Whether calls with ``k`` right-hand sides use programmatic dependent launch."""

@@ -358,7 +358,7 @@ class B200Runtime:
         return _DeviceLevels(array=arr, keepalive=keep)
 
     # -- autotuning ------------------------------------------------------------------------------
-    TUNE_VARIANTS = (5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 0, 1, 4)
+    TUNE_VARIANTS = (5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16, 0, 1, 4)
 
     def _tune_direction(self, direction: Direction) -> tuple[int, int]:
         """Fastest (narrow variant, heavy variant) for ``direction`` on the first artifact at

@@ -1076,8 +1076,8 @@ __device__ __forceinline__ void entry_short_rows(const LevelArgs& a, int64_t blo
 
 // narrow_variant 14: CTAs [0, heavy_blocks) take the heavy rows (lean walk), the next
 // long_blocks the two-slot narrow rows, the rest the short rows.
-// NW warps per CTA: 8 (narrow_variant 14), or 4 (15: finer-grained CTAs at the same 40 warps
-// per SM).
+// NW warps per CTA: 8 (narrow_variant 14), 4 (15) or 2 (16): finer-grained CTAs at the same 40
+// warps per SM.
 template <typename T, int INIT, bool UPONLY, int CW, int NW = kNarrowWarps>
 __global__ void __launch_bounds__(32 * NW, 40 / NW) level_entry_pre_kernel(LevelArgs a, int64_t heavy_blocks, int64_t long_blocks) {
     pdl_trigger();
@@ -2310,7 +2310,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
-    if (variant == 13 || variant == 14 || variant == 15) {  // entry-parallel narrow rows where the shape allows it, else as 12
+    if (variant >= 13 && variant <= 16) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
         const bool common = lean && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE;
         // 32-byte chunks: k = 2^n chunks of C columns (the shape's V = C / 2 columns per lane)
@@ -2320,7 +2320,7 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         // k below a chunk: one chunk lane of the shape's V = k columns (the shape's alignment)
         const bool narrow_k = common && !chunks && V < C && la.log2g == 0 && la.k == V;
         if (chunks || narrow_k) {
-            const int nw = variant == 15 ? 4 : kNarrowWarps;  // warps per CTA; heavy rows: one each
+            const int nw = variant == 15 ? 4 : (variant == 16 ? 2 : kNarrowWarps);  // warps per CTA; heavy rows: one each
             const int64_t heavy_blocks = (la.num_heavy + nw - 1) / nw;
             const int lg = la.log2g + (chunks ? 0 : 1);  // log2 of a row's 2W lanes
             const int log2w = lg - 1;                    // one entry slot: W lanes per short row
@@ -2337,11 +2337,15 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
             } else if (variant == 14) {
                 if (chunks) { GRG_ENTRY(level_entry_pre_kernel, C) } else { GRG_ENTRY(level_entry_pre_kernel, V) }
             } else {
-#define GRG_ENTRY4(CW)                                                                                                        \
-    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_entry_pre_kernel<T, 0, true, CW, 4>, la, heavy_blocks, long_blocks)); \
-    else GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_entry_pre_kernel<T, 0, false, CW, 4>, la, heavy_blocks, long_blocks));
-                if (chunks) { GRG_ENTRY4(C) } else { GRG_ENTRY4(V) }
-#undef GRG_ENTRY4
+#define GRG_ENTRY_NW(CW, NW)                                                                                                        \
+    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, 32 * NW, level_entry_pre_kernel<T, 0, true, CW, NW>, la, heavy_blocks, long_blocks)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, 32 * NW, level_entry_pre_kernel<T, 0, false, CW, NW>, la, heavy_blocks, long_blocks));
+                if (variant == 15) {
+                    if (chunks) { GRG_ENTRY_NW(C, 4) } else { GRG_ENTRY_NW(V, 4) }
+                } else {
+                    if (chunks) { GRG_ENTRY_NW(C, 2) } else { GRG_ENTRY_NW(V, 2) }
+                }
+#undef GRG_ENTRY_NW
             }
 #undef GRG_ENTRY
             GRG_LAUNCH_CHECK("level_entry_kernel");

@@ -225,7 +225,7 @@ typedef struct grg_b200_traverse_args {
                                            first 4 quads loaded before the previous level ends.
                                            At k = V (k below a 32-byte chunk: k = 1, 2 in FP64)
                                            13 and 14 walk one V-column chunk lane per row;
-                                           15: as 14 in 4-warp (128-thread) CTAs.
+                                           15 and 16: as 14 in 4-warp and 2-warp CTAs.
                                            13 and 14 walk a level's short_rows with one entry
                                            slot (each lane adds its chunk of all 4 entries).
                                            11 to 14 fall back to 7 with an
@@ -279,7 +279,7 @@ typedef struct grg_b200_traverse_args {
 typedef enum grg_b200_schedule { GRG_B200_SCHEDULE_LEVELS = 0, GRG_B200_SCHEDULE_DATAFLOW = 1 } grg_b200_schedule;
 #define GRG_B200_DEVICE_WAIT_TIMEOUT 6
 
-#define GRG_B200_NARROW_VARIANTS 16
+#define GRG_B200_NARROW_VARIANTS 17
 
 /* Library ABI version (GRG_B200_ABI_VERSION of the build). */
 int grg_b200_abi_version(void);

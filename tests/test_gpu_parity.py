@@ -53,7 +53,7 @@ def _cases_by_artifact():
 GROUPS = _cases_by_artifact()
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16])
 @pytest.mark.parametrize("heavy", [128, 2], ids=["narrow", "heavy-rows"])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_bit_exact_in_exact_order(group, heavy, variant, golden_data):
@@ -130,7 +130,7 @@ def test_golden_mixed_precision(group, heavy, golden_data):
         assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("variant", [13, 14, 15])
+@pytest.mark.parametrize("variant", [13, 14, 15, 16])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_entry_walks_with_heavy_rows(group, variant, golden_data):
     """The entry-parallel walks with many heavy rows (threshold 4) in the same launch, and the
@@ -154,7 +154,7 @@ def test_golden_entry_walks_with_heavy_rows(group, variant, golden_data):
         assert runtime.device_error() == 0
 
 
-@pytest.mark.parametrize("variant", [11, 12, 13, 14, 15])
+@pytest.mark.parametrize("variant", [11, 12, 13, 14, 15, 16])
 @pytest.mark.parametrize("group", sorted(GROUPS), ids=[f"{a}-{d}" for a, d in sorted(GROUPS)])
 def test_golden_lean_walks(group, variant, golden_data):
     """The lean walks on every golden case (no bounds-check word, rows not split, no heavy

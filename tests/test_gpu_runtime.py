@@ -663,7 +663,7 @@ def test_lean_walks_match_variant_7_and_the_oracle(synth_artifact, k):
 
     oracle = OracleGRG(synth_artifact)
     results = {}
-    for variant in (7, 11, 12, 13, 14, 15):
+    for variant in (7, 11, 12, 13, 14, 15, 16):
         plan = B200Plan(narrow_variant=variant, heavy_threshold=24, heavy_variant=2, narrow_split=0)
         layout = _layout([synth_artifact], requirements=_req(k=max(k, 2)), pair=B200PlanPair(plan_up=plan, plan_down=plan))
         rng = np.random.default_rng(300 + k)  # the same inputs for every variant
@@ -690,11 +690,12 @@ def test_lean_walks_match_variant_7_and_the_oracle(synth_artifact, k):
             out.append(("int", grg.matmul(xd, "down", by_individual=True, miss=miss.copy()),
                         oracle.matmul(xd, "down", by_individual=True, miss=miss.copy())))
             results[variant] = out
-    for (kind, got7, ref), (_, got11, _), (_, got12, _), (_, got13, _), (_, got14, _), (_, got15, _) in zip(
-            results[7], results[11], results[12], results[13], results[14], results[15]):
+    for (kind, got7, ref), (_, got11, _), (_, got12, _), (_, got13, _), (_, got14, _), (_, got15, _), (_, got16, _) in zip(
+            results[7], results[11], results[12], results[13], results[14], results[15], results[16]):
         np.testing.assert_array_equal(got11, got7)
         np.testing.assert_array_equal(got14, got13)  # the same sums, codes loaded earlier
         np.testing.assert_array_equal(got15, got14)  # the same walk in 4-warp CTAs
+        np.testing.assert_array_equal(got16, got14)  # and in 2-warp CTAs
         if kind == "int":
             np.testing.assert_array_equal(got12, ref)
             np.testing.assert_array_equal(got13, ref)

@@ -74,7 +74,7 @@ def test_invalid_arguments_fail_before_any_launch():
     args.k = 4
     args.ld_state = 4
     args.state = 16
-    args.narrow_variant = 16
+    args.narrow_variant = 17
     assert lib.grg_b200_traverse(ctypes.byref(args), None) == nat.ERR_INVALID
     assert "narrow_variant" in nat.last_error(lib)
 

@@ -200,7 +200,7 @@ def test_kernel_shape_options_validate_and_round_trip():
     with pytest.raises(ValueError, match="fuse_entries"):
         B200Plan(fuse_entries=-5)
     with pytest.raises(ValueError, match="narrow_variant"):
-        B200Plan(narrow_variant=16)
+        B200Plan(narrow_variant=17)
     with pytest.raises(ValueError, match="padded"):
         B200Plan(narrow_variant=9, pad_lists=False)
     plan = B200Plan.from_dict({"narrow_variant": 10, "persist_ctas": 3, "fuse_entries": 600_000, "pdl": False})
