@@ -239,12 +239,12 @@ def measured_peak_hbm() -> tuple[float, str]:
 # k = 8, FP64, default plan, measured with ncu -c 1 and L2 left warm (profiles/
 # level_traffic_config2_k8.md gives the commands).  Keys: (direction, level).
 CONFIG2_K8_TRAFFIC = {
-    ("up", 1): {"kernel": "level_entry_pre_kernel", "dram_bytes": 12050176 + 50176, "ncu_us": 24.42},
-    ("down", 3): {"kernel": "level_entry_pre_kernel", "dram_bytes": 127365888 + 22688512, "ncu_us": 34.98},
-    ("down", 1): {"kernel": "level_entry_pre_kernel", "dram_bytes": 524657152 + 21673984, "ncu_us": 115.74},
-    ("down", 0): {"kernel": "level_lean_warp_kernel", "dram_bytes": 457806336 + 16741120, "ncu_us": 208.93},
+    ("up", 1): {"kernel": "level_entry_pre_kernel", "dram_bytes": 12052480 + 45312, "ncu_us": 24.58},
+    ("down", 3): {"kernel": "level_entry_pre_kernel", "dram_bytes": 126545664 + 20910848, "ncu_us": 33.73},
+    ("down", 1): {"kernel": "level_entry_pre_kernel", "dram_bytes": 525780224 + 21631744, "ncu_us": 110.72},
+    ("down", 0): {"kernel": "level_lean_warp_kernel", "dram_bytes": 458001152 + 17115392, "ncu_us": 208.93},
 }
-CONFIG2_K8_VARIANT = 14  # the narrow variant those launches ran
+CONFIG2_K8_VARIANT = 15  # the narrow variant those launches ran
 TRAFFIC_SOURCE = "profiles/level_traffic_config2_k8.md (ncu -c 1 per launch on the config-2 graph, k = 8)"
 
 
