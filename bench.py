@@ -470,7 +470,7 @@ def run_b200(args) -> None:
                 if pair.plan_down.schedule == "dataflow":
                     level_launches += 3 if name == "up" else 2  # sentinel fill (+ seed) + dataflow kernel + output
                 else:
-                    fused = op._args.heavy_variant in (2, 4, 5) and op._args.narrow_variant >= 6 and not op._args.exact_order
+                    fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                     lv_arr = runtime._artifacts[0].levels[op._spec.direction].array
                     level_launches += traversal_level_launches(lv_arr, fused, int(op._args.fuse_entries)) + (2 if name == "up" else 1)
                 lv_order = range(1, scan.num_levels) if name == "up" else range(scan.num_levels - 1, -1, -1)
@@ -488,7 +488,7 @@ def run_b200(args) -> None:
             for i in range(levels.count):
                 nat.check(lib, lib.grg_b200_run_level(ctypes.byref(args_c), ctypes.byref(levels.array[i]),
                                                       ctypes.c_void_p(stream.cuda_stream)), "run_level")
-                fused = op._args.heavy_variant in (2, 4, 5) and op._args.narrow_variant >= 6 and not op._args.exact_order
+                fused = op._args.heavy_variant == 2 and op._args.narrow_variant >= 6 and not op._args.exact_order
                 lv = levels.array[i]
                 level_launches += 1 + (1 if 0 < lv.num_heavy < lv.num_rows and not fused else 0)
             b.record(stream)

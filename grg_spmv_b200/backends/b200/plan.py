@@ -74,10 +74,8 @@ class B200Plan:
     ``heavy_variant``).
     ``pad_lists``: pad every gather list to a multiple of 4 entries (needed by variant 6).
     ``heavy_variant``: heavy rows one CTA each (0), one warp each (1), or one warp each inside
-    the narrow-row launch (2, with ``narrow_variant`` 6 or 7); 3 as 1 with 32 rows per CTA;
-    4 and 5 as 2, with all-heavy levels of the lean walks 4 and 2 rows per CTA; None picks 2
-    with the padded variants and otherwise 1 for k <= 16, 0 above.  Exact order always uses
-    CTAs.
+    the narrow-row launch (2, with ``narrow_variant`` 6 or 7); None picks 2 with the padded
+    variants and otherwise 1 for k <= 16, 0 above.  Exact order always uses CTAs.
     ``long_first``: with ``balance``, the longest length bucket is processed first.
     ``pdl``: launch the level, seed and output kernels with programmatic dependent launch
     (each overlaps the end of the previous one; ignored when levels are streamed).  None turns
@@ -134,8 +132,8 @@ class B200Plan:
             raise ValueError(f"narrow_variant must be in [0, {nat.NARROW_VARIANTS}), got {self.narrow_variant}")
         if self.narrow_variant is not None and int(self.narrow_variant) >= 6 and not self.pad_lists:
             raise ValueError(f"narrow_variants 6-{nat.NARROW_VARIANTS - 1} read padded gather lists; they need pad_lists=True")
-        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3, 4, 5):
-            raise ValueError(f"heavy_variant must be 0 to 5, got {self.heavy_variant}")
+        if self.heavy_variant is not None and int(self.heavy_variant) not in (0, 1, 2, 3):
+            raise ValueError(f"heavy_variant must be 0, 1, 2 or 3, got {self.heavy_variant}")
         if not -1 <= int(self.narrow_split) <= 3:
             raise ValueError(f"narrow_split must be in [-1, 3], got {self.narrow_split}")
         if self.schedule not in ("levels", "dataflow"):

@@ -1106,12 +1106,11 @@ __global__ void __launch_bounds__(kNarrowThreads, 5) level_lean_kernel(LevelArgs
     else lean_rows<T, V, INIT, SEG, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
 }
 
-// All-heavy levels under narrow_variants 11 to 16: the lean heavy walk alone, WPC rows (warps)
-// per CTA: 8, or 4 and 2 with heavy_variant 4 and 5 (finer-grained CTAs).
-template <typename T, int V, int INIT, bool UPONLY, int WPC = kWarpRowThreads / 32>
-__global__ void __launch_bounds__(32 * WPC) level_lean_warp_kernel(LevelArgs a) {
+// All-heavy levels under narrow_variant 11 / 12: the lean heavy walk alone.
+template <typename T, int V, int INIT, bool UPONLY>
+__global__ void __launch_bounds__(kWarpRowThreads) level_lean_warp_kernel(LevelArgs a) {
     pdl_trigger();
-    lean_heavy_rows<T, V, INIT, UPONLY, WPC>(a, blockIdx.x);
+    lean_heavy_rows<T, V, INIT, UPONLY>(a, blockIdx.x);
 }
 
 // Narrow rows of padded lists, persistent (narrow_variant 9 and 10).  The narrow CTAs of a
@@ -2209,7 +2208,7 @@ int validate_common(const grg_b200_traverse_args* a) {
     if (a->init_mode < 0 || a->init_mode > 3) return fail(GRG_B200_ERR_INVALID, "unknown init_mode %d", a->init_mode);
     if (a->narrow_variant < 0 || a->narrow_variant >= GRG_B200_NARROW_VARIANTS)
         return fail(GRG_B200_ERR_INVALID, "narrow_variant %d outside [0, %d)", a->narrow_variant, GRG_B200_NARROW_VARIANTS);
-    if (a->heavy_variant < 0 || a->heavy_variant > 5) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 5]", a->heavy_variant);
+    if (a->heavy_variant < 0 || a->heavy_variant > 3) return fail(GRG_B200_ERR_INVALID, "heavy_variant %d outside [0, 3]", a->heavy_variant);
     if (a->narrow_split < -1 || a->narrow_split > 3) return fail(GRG_B200_ERR_INVALID, "narrow_split %d outside [-1, 3]", a->narrow_split);
     if (a->persist_ctas < 0) return fail(GRG_B200_ERR_INVALID, "persist_ctas must be >= 0, got %d", a->persist_ctas);
     if (a->fuse_entries < 0) return fail(GRG_B200_ERR_INVALID, "fuse_entries must be >= 0, got %lld", (long long)a->fuse_entries);
@@ -2307,10 +2306,7 @@ template <typename T, int V>
 int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int variant, int heavy_variant, int persist_ctas, bool pdl,
                        cudaStream_t s) {
     const int64_t narrow = la.num_rows - la.num_heavy;  // heavy positions form the suffix
-    // heavy_variant 4 and 5: as 2, with all-heavy levels of the lean walks 4 or 2 rows per CTA
-    const int heavy_wpc = heavy_variant == 4 ? 4 : (heavy_variant == 5 ? 2 : kWarpRowThreads / 32);
-    if (heavy_variant >= 4) heavy_variant = 2;
-    // the lean walks (11 to 16) serve launches without an error word and without row splits;
+    // the lean walks (11, 12) serve launches without an error word and without row splits;
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
@@ -2372,18 +2368,6 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
             }
 #undef GRG_LEAN
             GRG_LAUNCH_CHECK("level_lean_kernel");
-            return GRG_B200_OK;
-        }
-        if (lean && narrow == 0 && la.num_heavy > 0 && heavy_wpc != kWarpRowThreads / 32 && init_mode == 0) {
-            const dim3 grid(static_cast<unsigned>((la.num_heavy + heavy_wpc - 1) / heavy_wpc));
-            if (heavy_wpc == 4) {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_lean_warp_kernel<T, V, 0, true, 4>, la));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_lean_warp_kernel<T, V, 0, false, 4>, la));
-            } else {
-                if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, 64, level_lean_warp_kernel<T, V, 0, true, 2>, la));
-                else GRG_CUDA_TRY(launch_k(pdl, s, grid, 64, level_lean_warp_kernel<T, V, 0, false, 2>, la));
-            }
-            GRG_LAUNCH_CHECK("level_lean_warp_kernel");
             return GRG_B200_OK;
         }
         if (lean && narrow == 0 && la.num_heavy > 0) {

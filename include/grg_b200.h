@@ -236,10 +236,8 @@ typedef struct grg_b200_traverse_args {
                                            warp per row (lane groups split the list, shuffle
                                            reduction); 2 as 1 but in the same launch as the narrow
                                            rows (narrow_variant 6 to 10 only; otherwise as 1); 3 as 1
-                                           with 32 heavy rows (1024 threads) per CTA; 4 and 5
-                                           as 2, with all-heavy levels of the lean walks
-                                           (narrow_variant 11 to 16, no init) 4 and 2 rows per
-                                           CTA.  Exact order always uses one CTA per row. */
+                                           with 32 heavy rows (1024 threads) per CTA.  Exact
+                                           order always uses one CTA per row. */
     void* mix_scratch;                  /* GRG_B200_MIXED down: room for the encoded input, then
                                            (use_miss) the encoded miss rows, each a mixed buffer of
                                            num_mutations rows and ld_state columns */

@@ -115,7 +115,7 @@ def test_plan_options_validate():
     with pytest.raises(ValueError):
         B200PlanPair(plan_up=None, plan_down=None)
     with pytest.raises(ValueError):
-        B200Plan(heavy_variant=6)
+        B200Plan(heavy_variant=4)
     assert B200Plan.from_dict({"heavy_variant": 1}).heavy_variant == 1
     assert B200Plan().locality(Direction.DOWN) and not B200Plan().locality(Direction.UP)
 
