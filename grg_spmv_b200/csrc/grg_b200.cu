@@ -745,12 +745,12 @@ __device__ __forceinline__ const T* lean_source(const LevelArgs& a, uint32_t cod
     }
 }
 
-template <typename T, int V, int INIT, bool SEG, bool UPONLY>
+template <typename T, int V, int INIT, bool SEG, bool UPONLY, int NW = kNarrowWarps>
 __device__ __forceinline__ void lean_rows(const LevelArgs& a, int64_t block) {
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t narrow = a.num_rows - a.num_heavy;  // heavy positions form the suffix
-    const int64_t pos = ((block * kNarrowWarps + warp) << (5 - a.log2g)) + (lane >> a.log2g);
+    const int64_t pos = ((block * NW + warp) << (5 - a.log2g)) + (lane >> a.log2g);
     if (pos >= narrow) return;  // no warp-wide operations below
     const int32_t q0 = __ldg(a.row_ptr + pos) >> 2;
     const int32_t q1 = __ldg(a.row_ptr + pos + 1) >> 2;
@@ -1099,11 +1099,12 @@ __global__ void __launch_bounds__(kNarrowThreads, 5) level_entry_kernel(LevelArg
 
 // narrow_variant 11 (SEG) / 12: heavy rows first, one warp each, then the narrow rows, as
 // level_fused_kernel; MB = 5 CTAs per SM.
-template <typename T, int V, int INIT, bool SEG, bool UPONLY>
-__global__ void __launch_bounds__(kNarrowThreads, 5) level_lean_kernel(LevelArgs a, int64_t heavy_blocks) {
+// NW warps per CTA: 8, or 4 where variants 15 and 16 fall back to 12.
+template <typename T, int V, int INIT, bool SEG, bool UPONLY, int NW = kNarrowWarps>
+__global__ void __launch_bounds__(32 * NW, 40 / NW) level_lean_kernel(LevelArgs a, int64_t heavy_blocks) {
     pdl_trigger();
-    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, V, INIT, UPONLY>(a, blockIdx.x);
-    else lean_rows<T, V, INIT, SEG, UPONLY>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
+    if (static_cast<int64_t>(blockIdx.x) < heavy_blocks) lean_heavy_rows<T, V, INIT, UPONLY, NW>(a, blockIdx.x);
+    else lean_rows<T, V, INIT, SEG, UPONLY, NW>(a, static_cast<int64_t>(blockIdx.x) - heavy_blocks);
 }
 
 // All-heavy levels under narrow_variant 11 / 12: the lean heavy walk alone.
@@ -2310,6 +2311,8 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
     // others fall back to variant 7's kernels
     const bool lean = variant >= 11 && la.err == nullptr && !exact && heavy_variant == 2 &&
                       la.ld_state < (int64_t{1} << 32) && la.ld_x < (int64_t{1} << 32) && la.ld_miss < (int64_t{1} << 32);
+    // variants 15 and 16 fall back to 12 in 4-warp CTAs, the others in 8-warp ones
+    const int fallback_nw = variant == 15 || variant == 16 ? 4 : kNarrowWarps;
     if (variant >= 13 && variant <= 16) {  // entry-parallel narrow rows where the shape allows it, else as 12
         constexpr int C = Chunk32<T>::C;
         const bool common = lean && narrow > 0 && la.log2s == 0 && init_mode == GRG_B200_INIT_NONE;
@@ -2354,6 +2357,23 @@ int launch_level_typed(const LevelArgs& la, int init_mode, bool exact, int varia
         variant = 12;
     }
     if (variant == 11 || variant == 12) {
+        if (lean && narrow > 0 && la.log2s == 0 && variant == 12 && fallback_nw == 4) {
+            const int64_t heavy_blocks = (la.num_heavy + 3) / 4;
+            const int64_t warps = (narrow + (32 >> la.log2g) - 1) >> (5 - la.log2g);
+            const dim3 grid(static_cast<unsigned>(heavy_blocks + (warps + 3) / 4));
+#define GRG_LEAN4(INIT)                                                                                                   \
+    if (la.up) GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_lean_kernel<T, V, INIT, false, true, 4>, la, heavy_blocks)); \
+    else GRG_CUDA_TRY(launch_k(pdl, s, grid, 128, level_lean_kernel<T, V, INIT, false, false, 4>, la, heavy_blocks));
+            switch (init_mode) {
+                case 0: GRG_LEAN4(0) break;
+                case 1: GRG_LEAN4(1) break;
+                case 2: GRG_LEAN4(2) break;
+                default: GRG_LEAN4(3) break;
+            }
+#undef GRG_LEAN4
+            GRG_LAUNCH_CHECK("level_lean_kernel");
+            return GRG_B200_OK;
+        }
         if (lean && narrow > 0 && la.log2s == 0) {
             constexpr int rows_per_cta = kWarpRowThreads / 32;
             const int64_t heavy_blocks = (la.num_heavy + rows_per_cta - 1) / rows_per_cta;
